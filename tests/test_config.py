@@ -1,0 +1,48 @@
+"""LB3D namelist input: reader, defaults and derived values
+(code/lb3d_config.F90)."""
+import os
+
+import pytest
+
+from lb3d_b200.config import Params, parse_namelists, read_input
+from tests._fixtures import GOLDEN
+
+
+def test_quoted_slash_and_comments():
+    g = parse_namelists("""
+&variable_input
+folder = './output/x'  ! a comment with / slash
+beta = 10.000000, fr = 0.7
+sci_od = .true.
+/
+""")
+    v = g["variable_input"]
+    assert v["folder"] == "./output/x"
+    assert v["beta"] == 10.0 and v["fr"] == 0.7 and v["sci_od"] is True
+
+
+def test_differential_file_overrides():
+    p = read_input(os.path.join(GOLDEN, "gyroid", "gyroid.in"),
+                   os.path.join(GOLDEN, "gyroid", "dump_xdr.din"))
+    assert p.dump_format == "xdr"
+    assert p.beta == 10.0 and p.g_ss == -0.003 and p.bdist == 2
+    assert p.restore == 1 and p.init_cond == 7
+
+
+def test_defaults_and_derived():
+    p = read_input(os.path.join(GOLDEN, "wettingWall", "wettingWall.in"), ncomp=2)
+    # rock_colour = 1.0 -> rock_colour_r (code/lb3d_config.F90:661-664)
+    assert p.rock_colour_r == 1.0 and p.rock_colour_b == 0.0
+    # g_accn_max* default to the lattice size (code/lb3d_config.F90:931-933)
+    assert (p.g_accn_max, p.g_accn_max_x, p.g_accn_max_y) == (16, 16, 16)
+    assert p.has_rock_file and p.obs_file == "wettingWall.wall.xdr"
+    assert Params().tau_d == 2.0 and Params().beta == 1.0
+
+
+def test_lees_edwards_flag_and_validation():
+    p = read_input(os.path.join(GOLDEN, "leesEdwards", "leesEdwards.in"), ncomp=2)
+    assert p.lees_edwards and p.shear_u == 0.01
+    p.validate()
+    p.ncomp = 3
+    with pytest.raises(ValueError, match="Lees Edwards"):
+        p.validate()
