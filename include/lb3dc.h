@@ -1,0 +1,187 @@
+/*
+ * lb3dc.h -- C ABI of the B200 (sm_100a) implementation of LB3D's
+ * per-timestep hot path.
+ *
+ * The entry points mirror the calls LB3D's time loop makes
+ * (code/lb3d_time_loop.F90:58-92):
+ *
+ *     lb3d_force_apply(6); lb3d_bc_apply(6)      -> lb3dc_force_apply, lb3dc_bc_apply
+ *     lb3d_advection                             -> lb3dc_advection
+ *     lb3d_bc_apply(8); lb3d_force_apply(8)      -> lb3dc_bc_apply, lb3dc_force_apply
+ *     lb3d_collision                             -> lb3dc_collision
+ *
+ * plus the state transfer a Fortran ISO_C_BINDING shim needs to hand its
+ * lattice (whole_N, code/lb3d_lattice.F90:235-239,274-287) to the device and
+ * back.  Plain pointers and sizes only; every function returns an int status
+ * (0 = LB3DC_OK, negative = error) and the message of the last error of a
+ * handle is available from lb3dc_last_error.
+ *
+ * Threading: one host thread per handle; each handle owns one CUDA stream.
+ * Calls are asynchronous on that stream except the ones documented as
+ * synchronising (downloads, reductions, dumps, lb3dc_sync).
+ */
+#ifndef LB3DC_H
+#define LB3DC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define LB3DC_OK 0
+#define LB3DC_EINVAL (-22)   /* bad argument or unsupported parameter set */
+#define LB3DC_ENOMEM (-12)   /* device or host allocation failed          */
+#define LB3DC_ECUDA (-5)     /* a CUDA runtime call failed                */
+#define LB3DC_ETIMEOUT (-110)/* a bounded device-side wait gave up        */
+#define LB3DC_ENAN (-33)     /* non-finite populations detected           */
+#define LB3DC_ENOTSUP (-95)  /* valid request this build does not support */
+#define LB3DC_ESTATE (-71)   /* call out of order (e.g. no state loaded)  */
+
+/* ---- precision modes ------------------------------------------------- */
+#define LB3DC_FP64 0         /* plain drop-in: FP64 populations, FP64 math */
+#define LB3DC_FP32_DEV 1     /* FP32 storage of n - w_i rho0, FP32 collide */
+
+/*
+ * Hot-path parameters: the &fixed_input / &variable_input / &lbe_input
+ * scalars that the per-step path reads (code/lb3d_config.F90:44-297), after
+ * the reference's derived-value rules (rock_colour -> rock_colour_r/_b,
+ * g_accn_max* defaults; code/lb3d_config.F90:661-664,931-933).
+ * Component order: red, blue, surfactant.  ncomp is 2 (the reference's
+ * -DNOSURFACTANT build) or 3 (its default ternary build).
+ */
+typedef struct lb3dc_params {
+  int nx, ny, nz, ncomp;
+  double tau_r, tau_b, tau_s, tau_d;
+  double amass_r, amass_b, amass_s;
+  double g_br, g_bs, g_ss, g_wr, g_wb, tau_wr, tau_wb;
+  double beta, d_0;
+  double g_accn, g_accn_x, g_accn_y;
+  int g_accn_min, g_accn_max, g_accn_min_x, g_accn_max_x, g_accn_min_y, g_accn_max_y;
+  double shear_u, shear_omega;
+  int boundary_cond, inv_fluid;
+  double rock_colour_r, rock_colour_b;
+  int bdist;    /* must be 2 (the third-order equilibrium)               */
+  int restore;  /* 1 when the state comes from a checkpoint (init_cond 7) */
+  int precision;/* LB3DC_FP64 or LB3DC_FP32_DEV                           */
+  double rho0;  /* reference density of the FP32 deviation storage        */
+} lb3dc_params;
+
+typedef struct lb3dc_handle lb3dc_handle;
+
+/* ---- lifetime --------------------------------------------------------- */
+/* Validates p (the fatal combinations of code/lb3d_compatibility.F90:105-111
+ * are rejected with LB3DC_EINVAL), allocates the device lattice on the
+ * current CUDA device.  Replaces the allocation of whole_N
+ * (code/lb3d_lattice.F90:274-287). */
+int lb3dc_create(const lb3dc_params *p, lb3dc_handle **out);
+int lb3dc_destroy(lb3dc_handle *h);
+/* Copies the last error message of h (or of the last failed lb3dc_create
+ * when h is NULL) into buf; returns the status code of that error. */
+int lb3dc_last_error(const lb3dc_handle *h, char *buf, int len);
+/* Bytes of device memory the handle holds. */
+long long lb3dc_device_bytes(const lb3dc_handle *h);
+/* Device bytes a handle with these parameters would allocate. */
+long long lb3dc_footprint(const lb3dc_params *p);
+
+/* ---- state transfer (synchronising) ----------------------------------- */
+/*
+ * Loads a restored lattice and performs what the reference does after a
+ * restore: zero populations at rock sites and colour them
+ * (lbe_init_rock_colour, code/lb3d_ic_rock.F90:146-189), then
+ * lb3d_bc_init(4) (code/lb3d_bc.F90:48-90: the Lees-Edwards shear_u
+ * correction and shear_sum bookkeeping).
+ *   n    : [ncomp][19][nz][ny][nx] populations, x fastest
+ *   db   : [3][nz][ny][nx] surfactant dipoles (ternary; NULL for binary)
+ *   rock : [nz][ny][nx] rock_state (nonzero = rock; NULL = no rock)
+ *   shear_sum : value from the checktopo file; nt : restored time step.
+ */
+int lb3dc_upload_state(lb3dc_handle *h, const double *n, const double *db, const double *rock,
+                       double shear_sum, int nt);
+/* Interior state after the last completed call.  Any pointer may be NULL.
+ *   n, db as above; rho: [ncomp][site]; mom: [ncomp][3][site] (the
+ *   reference's u_* fields hold momentum); da: [3][site]. */
+int lb3dc_download_state(lb3dc_handle *h, double *n, double *db, double *rho, double *mom,
+                         double *da);
+/*
+ * The reference's own arena: whole_N(0:nx+1,0:ny+1,0:nz+1) of type lbe_site
+ * (code/lb3d_lattice.F90:35-83), sequence layout per site
+ *   per component: n(19), rho, u(3), rock_colour   then (ternary) da(3),
+ *   db(3)                                           then rock_state
+ * i.e. 49 (binary) or 79 (ternary) doubles per site, x fastest, halo 1.
+ * upload reads n, db and rock_state of the interior sites; download writes
+ * n, rho, u, rock_colour, da, db and rock_state of the interior sites.
+ */
+int lb3dc_upload_sites(lb3dc_handle *h, const double *whole_N, double shear_sum, int nt);
+int lb3dc_download_sites(lb3dc_handle *h, double *whole_N);
+
+/* ---- the time-loop stages (asynchronous) ------------------------------ */
+/* code/lb3d_force.F90:98-121: stages 6, 8, 10 are no-ops in the default
+ * build; kept for call-for-call parity. */
+int lb3dc_force_apply(lb3dc_handle *h, int stage);
+/* code/lb3d_bc.F90:95-155.  Stage 6 advances the time step counter and,
+ * under Lees-Edwards, updates shear_u, shear_sum and the plane offset and
+ * builds the x-halo; stage 8 rebuilds the Lees-Edwards halo after
+ * streaming.  Periodic halos are an index wrap inside the kernels. */
+int lb3dc_bc_apply(lb3dc_handle *h, int stage);
+/* code/lb3d_advection.F90:40-151 with half-way bounce-back
+ * (code/lb3d_bc_bounce.F90:53-90). */
+int lb3dc_advection(lb3dc_handle *h);
+/* code/lb3d_collision.F90:41-291: dipole relaxation (ternary), Shan-Chen
+ * and body forces, BGK relaxation. */
+int lb3dc_collision(lb3dc_handle *h);
+/* nsteps full time steps (stages 6..9 each); may fuse stages. */
+int lb3dc_time_loop(lb3dc_handle *h, int nsteps);
+/* Waits for all work of h; reports deferred kernel errors. */
+int lb3dc_sync(lb3dc_handle *h);
+
+/* ---- Lees-Edwards bookkeeping (FP64 on the host) ---------------------- */
+int lb3dc_set_lees_edwards(lb3dc_handle *h, double shear_sum, double shear_u);
+int lb3dc_get_lees_edwards(const lb3dc_handle *h, double *shear_sum, double *shear_u);
+int lb3dc_get_timestep(const lb3dc_handle *h, int *nt);
+
+/* ---- observability (synchronising) ------------------------------------ */
+/* FP64 sums over fluid sites: mass[c] = sum rho_c, mom[k] = sum_c sum
+ * n_c g c_k (the conserved quantities of lbe_sanity_check,
+ * code/lb3d_sanity.F90:130-234).  Deterministic order. */
+int lb3dc_reduce_conservation(lb3dc_handle *h, double mass[3], double mom[3]);
+/* Counts non-finite and negative populations (code/lb3d_sanity.F90:79-130). */
+int lb3dc_sanity(lb3dc_handle *h, long long *n_nonfinite, long long *n_negative);
+/* Science dump fields at the current state (code/lb3d_io_dump_data.F90):
+ * "od", "wd", "sur", "vel", "rock" -> [site]; "dir", "arr" -> [site][3];
+ * FP64 values, site index x fastest. */
+int lb3dc_dump(lb3dc_handle *h, const char *field, double *out);
+
+/* ---- XDR files (big-endian, the reference's formats) ------------------ */
+/* Checkpoint file of one rank (code/lb3d_io_checkpoint.F90:790-873,
+ * 1084-1106): sites x outermost, z innermost; per site n_r(19), n_b(19),
+ * [n_s(19), da(3), db(3)], rock_state as FP64. Arrays as in upload. */
+int lb3dc_xdr_read_checkpoint(const char *path, int nx, int ny, int nz, int ncomp, double *n,
+                              double *db, double *rock);
+int lb3dc_xdr_write_checkpoint(const char *path, int nx, int ny, int nz, int ncomp,
+                               const double *n, const double *da, const double *db,
+                               const double *rock);
+/* checktopo file (code/lb3d_io_checkpoint.F90:741-779): cdims(3),
+ * ccoords(3*nprocs) as int32, then shear_sum as FP64. One rank. */
+int lb3dc_xdr_read_topo(const char *path, double *shear_sum);
+int lb3dc_xdr_write_topo(const char *path, double shear_sum);
+/* Obstacle file (code/lb3d_io_xdrf.F90:358-479): FP32 per site, x fastest;
+ * value > 0 is rock.  rock: [nz][ny][nx] 0/1. */
+int lb3dc_xdr_read_rock(const char *path, int nx, int ny, int nz, double *rock);
+int lb3dc_xdr_write_rock(const char *path, int nx, int ny, int nz, const double *rock);
+/* Dump files (code/lb3d_io_xdrf.F90:717-754, 872-912): ncomp_per_site
+ * values per site, z outermost, x fastest, FP32 (dump_double = 0) or FP64. */
+int lb3dc_xdr_write_field(const char *path, const double *v, long long nsites,
+                          int values_per_site, int dump_double);
+
+/* ---- self-test helpers ------------------------------------------------- */
+/* Evaluates the deterministic FP64 exp (fn 0), expm1 (1) or tanh (2) of
+ * the FP64 path on the host (device = 0) or on the current CUDA device
+ * (device = 1) for n values; used to prove host/device bit identity. */
+int lb3dc_detmath_eval(int fn, int device, const double *x, double *y, long long n);
+/* Library build string. */
+const char *lb3dc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

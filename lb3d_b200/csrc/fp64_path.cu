@@ -1,0 +1,766 @@
+// fp64_path.cu -- the FP64 drop-in path (LB3DC_FP64).
+//
+// Stage-by-stage kernels whose arithmetic is, expression for expression,
+// the FP64 restatement of the reference (the oracle): the same operation
+// order, no FMA contraction (this file is compiled with --fmad=false) and
+// the deterministic exp/tanh of detmath.h, so that the device reproduces
+// the host restatement bit for bit.  The 1e-12-after-1000-steps parity
+// target is below the chaotic amplification of a single rounding
+// difference, which is why bit identity is the design goal here.
+//
+// Layout in HBM (structure of arrays, site index x fastest):
+//   f, g   : [nc][19][nsites]  pre-stream state / post-stream populations
+//   rho    : [nc][nsites]      post-stream densities
+//   psi    : [nc][nsites]      1 - exp(-rho), evaluated once per site
+//   mom    : [nc][3][nsites]   post-stream momenta (the reference's u_*)
+//   da, db : [3][nsites]       advected dipole flux / dipoles (ternary)
+//   rock   : [nsites] uint8
+// Lees-Edwards x-halo planes (binary): [nc][19][nz][ny] pre-stream, and
+// [nc][nz][ny] densities after streaming.
+
+#include <cstdio>
+
+#include "common.cuh"
+#include "detmath.h"
+#include "fp64_path.h"
+
+namespace lb3d {
+namespace fp64 {
+
+using lb3d_detmath::det_exp;
+using lb3d_detmath::det_tanh;
+
+// Fortran max(a,b) for the clipping constants.
+__device__ __forceinline__ double fmaxf_(double a, double b) { return (a < b) ? b : a; }
+
+// The FP32 literals 10.e-5 and 10.e-9 widened to FP64
+// (code/lb3d_collision.F90:345,546,586).
+#define CLIP_RHO_S ((double)1.0e-4f)
+#define CLIP_RHO ((double)1.0e-8f)
+
+__device__ __forceinline__ double get_psi(double rho) { return 1.0 - det_exp(-rho); }
+
+// boltz_dist, bdist = 2, code/lb3d_bdist.F90:301-370.
+__device__ __forceinline__ void boltz2(double ux, double uy, double uz, double dux, double duy,
+                                       double duz, double *b) {
+  const double T = 1.0 / 3.0;
+  const double holdit = 1.0 / T;
+  const double w1 = 1.0 / 36.0;
+  const double w0 = 1.0 / 3.0;
+  double tux = ux + dux, tuy = uy + duy, tuz = uz + duz;
+  double tuxt = tux * holdit, tuyt = tuy * holdit, tuzt = tuz * holdit;
+  double uke = 0.5 * (tux * tuxt + tuy * tuyt + tuz * tuzt);
+  double cst = 1.0 - uke;
+  double c1 = w1 * cst;
+  double wb2 = w1 / 2.0, wb6 = w1 / 6.0;
+#define LB3D_PAIR(CD, I, J)                                 \
+  {                                                         \
+    double cdotu = (CD);                                    \
+    double even = c1 + wb2 * (cdotu * cdotu);               \
+    double odd = c1 * cdotu + wb6 * (cdotu * cdotu * cdotu); \
+    b[I] = even + odd;                                      \
+    b[J] = even - odd;                                      \
+  }
+  LB3D_PAIR(tuxt, 0, 1)
+  LB3D_PAIR(tuyt, 2, 3)
+  LB3D_PAIR(tuzt, 4, 5)
+  LB3D_PAIR(tuxt + tuyt, 6, 11)
+  LB3D_PAIR(tuxt - tuyt, 7, 10)
+  LB3D_PAIR(tuxt + tuzt, 8, 13)
+  LB3D_PAIR(tuxt - tuzt, 9, 12)
+  LB3D_PAIR(tuyt + tuzt, 14, 17)
+  LB3D_PAIR(tuyt - tuzt, 15, 16)
+#undef LB3D_PAIR
+  b[REST] = w0 * cst;
+}
+
+__device__ __forceinline__ void site_xyz(long long i, int nx, int ny, int &x, int &y, int &z) {
+  long long t = i / nx;
+  x = (int)(i - t * nx);
+  z = (int)(t / ny);
+  y = (int)(t - (long long)z * ny);
+}
+
+// ---------------------------------------------------------------------------
+// Lees-Edwards x-halo (code/lb3d_bc_leesedwards.F90:147-1315, one rank).
+// One thread per (y,z) builds both halo sites, the bottom one first: the
+// clipping branch of the top halo reads the adjusted bottom site
+// (:951-986).
+// ---------------------------------------------------------------------------
+template <int NC>
+__device__ void le_adjust(const DevParams &P, double h[NC][19], const double ref[NC][19],
+                          double shear_u, double sign) {
+  double p[NC][3], ns[NC];
+  for (int c = 0; c < NC; ++c) {
+    ns[c] = 0.0;
+    p[c][0] = p[c][1] = p[c][2] = 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < 19; ++q)
+    for (int c = 0; c < NC; ++c) {
+      ns[c] = ns[c] + h[c][q] * (double)gw(q);
+      double ng = h[c][q] * (double)gw(q);
+      p[c][0] = p[c][0] + ng * (double)cx(q);
+      p[c][1] = p[c][1] + ng * (double)cy(q);
+      p[c][2] = p[c][2] + ng * (double)cz(q);
+    }
+  double pt[3];
+  for (int k = 0; k < 3; ++k) pt[k] = (P.amass[0] * P.omega[0]) * p[0][k];
+  double rho_c = P.amass[0] * ns[0];
+  double rho_tilde = rho_c * P.omega[0];
+  for (int c = 1; c < NC; ++c) {
+    for (int k = 0; k < 3; ++k) pt[k] = pt[k] + (P.amass[c] * P.omega[c]) * p[c][k];
+    rho_c = P.amass[c] * ns[c];
+    rho_tilde = rho_tilde + rho_c * P.omega[c];
+  }
+  double rho_tmp = fmaxf_(rho_tilde, CLIP_RHO);
+  double ut[3];
+  for (int k = 0; k < 3; ++k) ut[k] = pt[k] / rho_tmp;
+  double b_udu[19], b_u[19];
+  double uz2 = (sign < 0.0) ? ((ut[2] - shear_u) - shear_u) : ((ut[2] + shear_u) + shear_u);
+  boltz2(ut[0], ut[1], uz2, 0.0, 0.0, 0.0, b_udu);
+  boltz2(ut[0], ut[1], ut[2], 0.0, 0.0, 0.0, b_u);
+  double df[NC][19];
+  bool neg = false;
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      df[c][q] = ns[c] * (b_udu[q] - b_u[q]);
+      if (h[c][q] + df[c][q] < 0.0) neg = true;
+    }
+  if (neg) {
+    double mn = ref[0][0];
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q) mn = fmin(mn, ref[c][q]);
+    double df_scale;
+    if (mn > 0.0) {
+      df_scale = -df[0][0] / ref[0][0];
+      for (int c = 0; c < NC; ++c)
+        for (int q = 0; q < 19; ++q) df_scale = fmaxf_(df_scale, -df[c][q] / ref[c][q]);
+    } else {
+      df_scale = 0.0;
+    }
+    if (fabs(df_scale) > 1.0) {
+      for (int c = 0; c < NC; ++c)
+        for (int q = 0; q < 19; ++q) h[c][q] = ref[c][q] + df[c][q] / df_scale;
+    } else {
+      for (int c = 0; c < NC; ++c)
+        for (int q = 0; q < 19; ++q) h[c][q] = ref[c][q];
+    }
+  } else {
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q) h[c][q] = h[c][q] + df[c][q];
+  }
+}
+
+// src: populations [NC][19][nsites].  Writes the halo planes and, when
+// rho_out is given, their densities and psi (for the force stencil).
+template <int NC>
+__global__ void k_le_halo(DevParams P, LEStep S, const double *__restrict__ src,
+                          double *__restrict__ hlo, double *__restrict__ hhi,
+                          double *__restrict__ rlo, double *__restrict__ rhi,
+                          double *__restrict__ plo, double *__restrict__ phi) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ny * nz) return;
+  const int y = t % ny, z = t / ny;
+  const long long N = P.nsites;
+  const double f = S.lefrac;
+  double hb[NC][19], ht[NC][19];
+  {
+    long long ia = sidx(nx - 1, y, ((z + S.eoff) % nz + nz) % nz, nx, ny);
+    long long ib = sidx(nx - 1, y, ((z + S.eoff + 1) % nz + nz) % nz, nx, ny);
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q)
+        hb[c][q] = (1.0 - f) * src[(c * 19 + q) * N + ia] + f * src[(c * 19 + q) * N + ib];
+    le_adjust<NC>(P, hb, hb, S.shear_u, -1.0);
+  }
+  {
+    long long ia = sidx(0, y, ((z - S.eoff - 1) % nz + nz) % nz, nx, ny);
+    long long ib = sidx(0, y, ((z - S.eoff) % nz + nz) % nz, nx, ny);
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q)
+        ht[c][q] = f * src[(c * 19 + q) * N + ia] + (1.0 - f) * src[(c * 19 + q) * N + ib];
+    le_adjust<NC>(P, ht, hb, S.shear_u, +1.0);
+  }
+  const long long NP = (long long)ny * nz;
+  if (hlo) {
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q) {
+        hlo[(c * 19 + q) * NP + t] = hb[c][q];
+        hhi[(c * 19 + q) * NP + t] = ht[c][q];
+      }
+  }
+  if (rlo) {
+    for (int c = 0; c < NC; ++c) {
+      double a = 0.0, b = 0.0;
+#pragma unroll
+      for (int q = 0; q < 19; ++q) {
+        a = a + hb[c][q] * (double)gw(q);
+        b = b + ht[c][q] * (double)gw(q);
+      }
+      rlo[c * NP + t] = a;
+      rhi[c * NP + t] = b;
+      plo[c * NP + t] = get_psi(a);
+      phi[c * NP + t] = get_psi(b);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Advection: pull streaming with half-way bounce-back, the advected dipole
+// flux and the post-stream moments (code/lb3d_advection.F90:54-151,
+// code/lb3d_bc_bounce.F90:53-90, code/lb3d_analysis.F90:64-102).
+// ---------------------------------------------------------------------------
+template <int NC, bool LE>
+__global__ void __launch_bounds__(256) k_stream(DevParams P, const double *__restrict__ fin,
+                                                double *__restrict__ fout, double *__restrict__ rho,
+                                                double *__restrict__ psi, double *__restrict__ mom,
+                                                double *__restrict__ da,
+                                                const double *__restrict__ db,
+                                                const uint8_t *__restrict__ rock,
+                                                const double *__restrict__ hlo,
+                                                const double *__restrict__ hhi) {
+  const long long N = P.nsites;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int x, y, z;
+  site_xyz(i, nx, ny, x, y, z);
+  const bool fluid = rock[i] == 0;
+  const long long NP = (long long)ny * nz;
+
+  // upstream index of each moving direction: -1/-2 mark the LE halos
+  long long up[18];
+  bool upf[18];
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    int xu = x - cx(q), yu = wrap(y - cy(q), ny), zu = wrap(z - cz(q), nz);
+    if (LE && xu < 0) {
+      up[q] = -1 - (yu + (long long)ny * zu);  // bottom halo
+      upf[q] = true;
+    } else if (LE && xu >= nx) {
+      up[q] = -1 - NP - (yu + (long long)ny * zu);  // top halo
+      upf[q] = true;
+    } else {
+      up[q] = sidx(wrap(xu, nx), yu, zu, nx, ny);
+      upf[q] = rock[up[q]] == 0;
+    }
+  }
+  auto pulled = [&](int c, int q) -> double {
+    long long j = up[q];
+    if (LE && j < 0) {
+      long long h = -1 - j;
+      if (h < NP) return hlo[(c * 19 + q) * NP + h];
+      return hhi[(c * 19 + q) * NP + (h - NP)];
+    }
+    return fin[(c * 19 + q) * N + j];
+  };
+
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  for (int c = 0; c < NC; ++c) {
+    double n[19];
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+      if (fluid)
+        n[q] = upf[q] ? pulled(c, q) : fin[(c * 19 + bounce(q)) * N + i];
+      else
+        n[q] = fin[(c * 19 + q) * N + i];
+    }
+    n[REST] = fin[(c * 19 + REST) * N + i];
+    if (NC == 3 && c == 2) {
+      // advected dipole flux: bounce-back terms first (lb3d_bc_bounce_back_hw
+      // runs before lb3d_advection_step), then the pulls, then the rest
+      // population (code/lb3d_advection.F90:137-148).
+      if (fluid) {
+#pragma unroll
+        for (int s = 0; s < 18; ++s) {
+          long long ja = sidx(wrap(x + cx(s), nx), wrap(y + cy(s), ny), wrap(z + cz(s), nz), nx, ny);
+          if (rock[ja] != 0) {
+            double ng = fin[(2 * 19 + s) * N + i] * (double)gw(s);
+            d0 = d0 + ng * db[ja];
+            d1 = d1 + ng * db[N + ja];
+            d2 = d2 + ng * db[2 * N + ja];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 18; ++q) {
+          if (upf[q]) {
+            long long j = up[q];
+            double ng = n[q] * (double)gw(q);
+            d0 = d0 + ng * db[j];
+            d1 = d1 + ng * db[N + j];
+            d2 = d2 + ng * db[2 * N + j];
+          }
+        }
+      }
+      double ng = n[REST] * (double)gw(REST);
+      d0 = d0 + ng * db[i];
+      d1 = d1 + ng * db[N + i];
+      d2 = d2 + ng * db[2 * N + i];
+    }
+    double r = 0.0, u0 = 0.0, u1 = 0.0, u2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      fout[(c * 19 + q) * N + i] = n[q];
+      r = r + n[q] * (double)gw(q);
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      double ng = n[q] * (double)gw(q);
+      u0 = u0 + ng * (double)cx(q);
+      u1 = u1 + ng * (double)cy(q);
+      u2 = u2 + ng * (double)cz(q);
+    }
+    rho[c * N + i] = r;
+    psi[c * N + i] = get_psi(r);
+    mom[(c * 3 + 0) * N + i] = u0;
+    mom[(c * 3 + 1) * N + i] = u1;
+    mom[(c * 3 + 2) * N + i] = u2;
+  }
+  if (NC == 3) {
+    da[i] = d0;
+    da[N + i] = d1;
+    da[2 * N + i] = d2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dipole relaxation, code/lb3d_collision.F90:296-403 (ternary, periodic).
+// Reads rho and da of the 18 neighbours; writes db in place (no neighbour
+// reads db in this pass).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_dipole(DevParams P, const double *__restrict__ rho,
+                                                const double *__restrict__ da,
+                                                double *__restrict__ db) {
+  const long long N = P.nsites;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int x, y, z;
+  site_xyz(i, nx, ny, x, y, z);
+  double h_c[3] = {0.0, 0.0, 0.0};
+  double h_s[3] = {da[i], da[N + i], da[2 * N + i]};
+  double sN_tmp = fmaxf_(rho[2 * N + i], CLIP_RHO_S);
+  double sd_tmp[3];
+  for (int k = 0; k < 3; ++k) sd_tmp[k] = h_s[k] / sN_tmp;
+  const double sgn = (P.g_bs >= 0.0) ? 1.0 : -1.0;
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    long long j = sidx(wrap(x + cx(q), nx), wrap(y + cy(q), ny), wrap(z + cz(q), nz), nx, ny);
+    double psi_r = 0.0 + rho[j];
+    double psi_b = 0.0 + rho[N + j];
+    double pas[3] = {da[j], da[N + j], da[2 * N + j]};
+    double hc_m = -(sgn * (psi_b - psi_r) * (double)gw(q));
+    const double c[3] = {(double)cx(q), (double)cy(q), (double)cz(q)};
+    for (int k = 0; k < 3; ++k) h_c[k] = h_c[k] + hc_m * c[k];
+    double hs_dot = 2.0 * ((c[0] * pas[0] + c[1] * pas[1]) + c[2] * pas[2]);
+    for (int k = 0; k < 3; ++k) h_s[k] = h_s[k] + (pas[k] - c[k] * hs_dot) * (double)gw(q);
+  }
+  double h[3];
+  for (int k = 0; k < 3; ++k) h[k] = h_c[k] + h_s[k];
+  double h_m = P.beta * sqrt((h[0] * h[0] + h[1] * h[1]) + h[2] * h[2]);
+  double sd_eq[3];
+  const double third = 1.0 / 3.0;
+  for (int k = 0; k < 3; ++k) sd_eq[k] = (third * P.beta) * h[k];
+  if (h_m > 10.0e-3) {
+    double exh = 1.0 / det_tanh(h_m);
+    double sd_mag = exh - 1.0 / h_m;
+    for (int k = 0; k < 3; ++k) sd_eq[k] = ((P.beta * h[k]) / h_m) * sd_mag;
+  }
+  for (int k = 0; k < 3; ++k) sd_eq[k] = sd_eq[k] * P.d_0;
+  for (int k = 0; k < 3; ++k) db[k * N + i] = P.omega_d * sd_eq[k] + (1.0 - P.omega_d) * sd_tmp[k];
+}
+
+// ---------------------------------------------------------------------------
+// Shan-Chen forces (code/lb3d_force_shanchen.F90:127-330).  LE selects the
+// Lees-Edwards neighbourhood: x-halo sites from the halo planes (never
+// rock), and rock neighbours reached through the y/z halo without their
+// rock colour (the Lees-Edwards y/z swaps do not copy it, :1079-1308).
+// ---------------------------------------------------------------------------
+template <bool LE>
+__device__ __forceinline__ void sc_force_binary(const DevParams &P, int x, int y, int z, long long i,
+                                                const double *__restrict__ rho,
+                                                const double *__restrict__ psi,
+                                                const uint8_t *__restrict__ rock,
+                                                const double *__restrict__ plo,
+                                                const double *__restrict__ phi, double *fr,
+                                                double *fb) {
+  const long long N = P.nsites;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const long long NP = (long long)ny * nz;
+  double f_br[3] = {0, 0, 0}, f_rb[3] = {0, 0, 0}, f_wr[3] = {0, 0, 0}, f_wb[3] = {0, 0, 0};
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    const double c[3] = {(double)cx(q), (double)cy(q), (double)cz(q)};
+    int xn = x + cx(q), yn = y + cy(q), zn = z + cz(q);
+    double psi_r, psi_b;
+    bool rk = false;
+    if (LE && (xn < 0 || xn >= nx)) {
+      long long h = wrap(yn, ny) + (long long)ny * wrap(zn, nz);
+      const double *pp = (xn < 0) ? plo : phi;
+      psi_r = pp[h];
+      psi_b = pp[NP + h];
+    } else {
+      long long j = sidx(wrap(xn, nx), wrap(yn, ny), wrap(zn, nz), nx, ny);
+      if (rock[j] != 0) {
+        rk = true;
+        bool through_halo = (yn < 0 || yn >= ny || zn < 0 || zn >= nz || xn < 0 || xn >= nx);
+        double rcr = (LE && through_halo) ? 0.0 : P.rc_r;
+        double rcb = (LE && through_halo) ? 0.0 : P.rc_b;
+        psi_r = get_psi(rho[j] + rcr);
+        psi_b = get_psi(rho[N + j] + rcb);
+      } else {
+        psi_r = psi[j];
+        psi_b = psi[N + j];
+      }
+    }
+    double green_r = psi_b * (double)gw(q);
+    double green_b = psi_r * (double)gw(q);
+    if (rk) {
+      for (int k = 0; k < 3; ++k) {
+        f_wb[k] = f_wb[k] + green_r * c[k];
+        f_wr[k] = f_wr[k] + green_b * c[k];
+      }
+    } else {
+      for (int k = 0; k < 3; ++k) {
+        f_rb[k] = f_rb[k] + green_r * c[k];
+        f_br[k] = f_br[k] + green_b * c[k];
+      }
+    }
+  }
+  double pb = psi[N + i], prr = psi[i];
+  for (int k = 0; k < 3; ++k) {
+    double br = -(P.g_br * f_br[k]);
+    double rb = -(P.g_br * f_rb[k]);
+    double wr = -(P.g_wr * f_wr[k]);
+    double wb = -(P.g_wb * f_wb[k]);
+    fb[k] = (br + ((wb / P.tau[1]) * P.tau_wb)) * pb;
+    fr[k] = (rb + ((wr / P.tau[0]) * P.tau_wr)) * prr;
+  }
+}
+
+__device__ __forceinline__ void sc_force_ternary(const DevParams &P, int x, int y, int z, long long i,
+                                                 const double *__restrict__ psi,
+                                                 const double *__restrict__ db, double *fr,
+                                                 double *fb, double *fs) {
+  const long long N = P.nsites;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  double f_br[3] = {0, 0, 0}, f_rb[3] = {0, 0, 0}, f_cs[3] = {0, 0, 0}, f_sc[3] = {0, 0, 0},
+         f_ss[3] = {0, 0, 0};
+  const double dbx[3] = {db[i], db[N + i], db[2 * N + i]};
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    long long j = sidx(wrap(x + cx(q), nx), wrap(y + cy(q), ny), wrap(z + cz(q), nz), nx, ny);
+    const double c[3] = {(double)cx(q), (double)cy(q), (double)cz(q)};
+    const double g = (double)gw(q);
+    double psi_r = psi[j];
+    double psi_b = psi[N + j];
+    double green_r = psi_b * g;
+    double green_b = psi_r * g;
+    for (int k = 0; k < 3; ++k) {
+      f_rb[k] = f_rb[k] + green_r * c[k];
+      f_br[k] = f_br[k] + green_b * c[k];
+    }
+    double pss = psi[2 * N + j];
+    double dd[3] = {db[j] * pss, db[N + j] * pss, db[2 * N + j] * pss};
+    double d_dotc = (dd[0] * c[0] + dd[1] * c[1]) + dd[2] * c[2];
+    for (int k = 0; k < 3; ++k) f_cs[k] = f_cs[k] + (dd[k] - (2.0 * d_dotc) * c[k]) * g;
+    double di_dotc = (dbx[0] * c[0] + dbx[1] * c[1]) + dbx[2] * c[2];
+    double greenc_s = (psi_b - psi_r) * g;
+    for (int k = 0; k < 3; ++k) f_sc[k] = f_sc[k] + greenc_s * (dbx[k] - (2.0 * di_dotc) * c[k]);
+    double di_dot_d = (dd[0] * dbx[0] + dd[1] * dbx[1]) + dd[2] * dbx[2];
+    double green_ss = 8.0 * g;
+    for (int k = 0; k < 3; ++k)
+      f_ss[k] = f_ss[k] +
+                green_ss * (((di_dot_d - (2.0 * di_dotc) * d_dotc) * c[k] + dd[k] * di_dotc) +
+                            d_dotc * dbx[k]);
+  }
+  double pb = psi[N + i], prr = psi[i], ps = psi[2 * N + i];
+  for (int k = 0; k < 3; ++k) {
+    double br = -(P.g_br * f_br[k]);
+    double rb = -(P.g_br * f_rb[k]);
+    double sc = (2.0 * P.g_bs) * f_sc[k];
+    double cs = -((2.0 * P.g_bs) * f_cs[k]);
+    double ss = -(P.g_ss * f_ss[k]);
+    fb[k] = (br + cs) * pb;
+    fr[k] = (rb - cs) * prr;
+    fs[k] = (sc + ss) * ps;
+  }
+}
+
+template <int NC, bool LE>
+__device__ __forceinline__ void sc_forces(const DevParams &P, int x, int y, int z, long long i,
+                                          const double *rho, const double *psi, const double *db,
+                                          const uint8_t *rock, const double *plo,
+                                          const double *phi, double F[NC][3]) {
+  for (int c = 0; c < NC; ++c) F[c][0] = F[c][1] = F[c][2] = 0.0;
+  if (rock[i] != 0) return;
+  if (NC == 2)
+    sc_force_binary<LE>(P, x, y, z, i, rho, psi, rock, plo, phi, F[0], F[1]);
+  else
+    sc_force_ternary(P, x, y, z, i, psi, db, F[0], F[1], F[NC - 1]);
+}
+
+// ---------------------------------------------------------------------------
+// Forces + BGK, code/lb3d_collision.F90:151-289.
+// ---------------------------------------------------------------------------
+template <int NC, bool LE>
+__global__ void __launch_bounds__(256) k_collide(DevParams P, const double *__restrict__ g,
+                                                 double *__restrict__ f,
+                                                 const double *__restrict__ rho,
+                                                 const double *__restrict__ psi,
+                                                 const double *__restrict__ mom,
+                                                 const double *__restrict__ db,
+                                                 const uint8_t *__restrict__ rock,
+                                                 const double *__restrict__ plo,
+                                                 const double *__restrict__ phi) {
+  const long long N = P.nsites;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int x, y, z;
+  site_xyz(i, P.nx, P.ny, x, y, z);
+  double F[NC][3];
+  sc_forces<NC, LE>(P, x, y, z, i, rho, psi, db, rock, plo, phi, F);
+  double r[NC];
+  for (int c = 0; c < NC; ++c) r[c] = rho[c * N + i];
+  if (applyforce(P, x + 1, y + 1, z + 1)) {
+    for (int c = 0; c < NC; ++c) {
+      double mass = P.amass[c] * r[c];
+      F[c][2] = F[c][2] + mass * P.g_accn;
+      F[c][1] = F[c][1] + mass * P.g_accn_y;
+      F[c][0] = F[c][0] + mass * P.g_accn_x;
+    }
+  }
+  double pt[3];
+  for (int k = 0; k < 3; ++k) pt[k] = (P.amass[0] * P.omega[0]) * mom[k * N + i];
+  for (int c = 1; c < NC; ++c)
+    for (int k = 0; k < 3; ++k) pt[k] = pt[k] + (P.amass[c] * P.omega[c]) * mom[(c * 3 + k) * N + i];
+  double rho_tilde = (P.amass[0] * r[0]) * P.omega[0];
+  for (int c = 1; c < NC; ++c) rho_tilde = rho_tilde + (P.amass[c] * r[c]) * P.omega[c];
+  double rt = fmaxf_(rho_tilde, CLIP_RHO);
+  double ut[3];
+  for (int k = 0; k < 3; ++k) ut[k] = pt[k] / rt;
+  for (int c = 0; c < NC; ++c) {
+    double pon = 1.0 / fmaxf_(r[c], CLIP_RHO);
+    double du[3];
+    for (int k = 0; k < 3; ++k) du[k] = ((P.tau[c] * pon) * F[c][k]) / P.amass[c];
+    double b[19];
+    boltz2(ut[0], ut[1], ut[2], du[0], du[1], du[2], b);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      double nq = g[(c * 19 + q) * N + i];
+      double eq = r[c] * b[q];
+      f[(c * 19 + q) * N + i] = nq - P.omega[c] * (nq - eq);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Science dumps (code/lb3d_io_dump_data.F90:922-1460).  The XDR dump path
+// gathers the lattice into a fresh arena with a plain periodic halo
+// (code/lb3d_io.F90:387-442, code/lb3d_mpi.F90:783-859), so the dump-time
+// forces always use the periodic neighbourhood.
+// ---------------------------------------------------------------------------
+template <int NC>
+__global__ void k_dump(DevParams P, int field, const double *__restrict__ f,
+                       const double *__restrict__ rho, const double *__restrict__ psi,
+                       const double *__restrict__ db, const uint8_t *__restrict__ rock,
+                       double *__restrict__ out) {
+  const long long N = P.nsites;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int x, y, z;
+  site_xyz(i, P.nx, P.ny, x, y, z);
+  const bool fluid = rock[i] == 0;
+  auto sumg = [&](int c, int dir) {
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      double cc = dir == 0 ? (double)cx(q) : dir == 1 ? (double)cy(q) : dir == 2 ? (double)cz(q) : 1.0;
+      acc = acc + (f[(c * 19 + q) * N + i] * (double)gw(q)) * cc;
+    }
+    return acc;
+  };
+  switch (field) {
+    case 0:  // od
+      out[i] = fluid ? P.amass[0] * sumg(0, 3) : 0.0;
+      break;
+    case 1:  // wd
+      out[i] = fluid ? P.amass[1] * sumg(1, 3) : 0.0;
+      break;
+    case 2:  // sur
+      out[i] = (NC == 3) ? P.amass[NC - 1] * sumg(NC - 1, 3) : 0.0;
+      break;
+    case 3:  // dir
+      for (int k = 0; k < 3; ++k) out[3 * i + k] = (NC == 3) ? db[k * N + i] : 0.0;
+      break;
+    case 4: {  // vel
+      if (fluid) {
+        double v = 0.0, den = 0.0;
+        for (int c = 0; c < NC; ++c) {
+          double term = (sumg(c, 2) * P.amass[c]) * P.omega[c];
+          v = (c == 0) ? term : v + term;
+          double dterm = (sumg(c, 3) * P.amass[c]) * P.omega[c];
+          den = (c == 0) ? dterm : den + dterm;
+        }
+        v = v / fmaxf_(10.0e-9, den);
+        if (in_accn_box(P, x + 1, y + 1, z + 1)) v = v - P.g_accn / 2.0;
+        out[i] = v;
+      } else {
+        out[i] = 0.0;
+      }
+      break;
+    }
+    case 5: {  // arr
+      double F[NC][3];
+      sc_forces<NC, false>(P, x, y, z, i, rho, psi, db, rock, nullptr, nullptr, F);
+      double den = 0.0;
+      for (int c = 0; c < NC; ++c) {
+        double t = sumg(c, 3) * P.amass[c];
+        den = (c == 0) ? t : den + t;
+      }
+      float dd = (float)den;
+      float denf = (1.0e-8f < dd) ? dd : 1.0e-8f;
+      for (int k = 0; k < 3; ++k) {
+        double v = 0.0;
+        for (int c = 0; c < NC; ++c) {
+          double m = sumg(c, k) * P.amass[c];
+          double corr = ((F[c][k] / 2.0) * sumg(c, 3)) * P.amass[c];
+          v = (c == 0) ? (m - corr) : ((v + m) - corr);
+        }
+        out[3 * i + k] = v / (double)denf;
+      }
+      if (in_accn_box(P, x + 1, y + 1, z + 1) && fluid) {
+        out[3 * i + 0] = out[3 * i + 0] - P.g_accn_x / 2.0;
+        out[3 * i + 1] = out[3 * i + 1] - P.g_accn_y / 2.0;
+        out[3 * i + 2] = out[3 * i + 2] - P.g_accn / 2.0;
+      }
+      break;
+    }
+    case 6:  // rock
+      out[i] = fluid ? 0.0 : 1.0;
+      break;
+  }
+}
+
+// Moments of the current state (used by downloads after a collision: the
+// reference's rho/u fields then still hold the post-stream moments, which
+// the stream kernel stored; this kernel is for states loaded by upload).
+template <int NC>
+__global__ void k_moments(DevParams P, const double *__restrict__ f, double *__restrict__ rho,
+                          double *__restrict__ psi, double *__restrict__ mom) {
+  const long long N = P.nsites;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int c = 0; c < NC; ++c) {
+    double r = 0.0, u0 = 0.0, u1 = 0.0, u2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) r = r + f[(c * 19 + q) * N + i] * (double)gw(q);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      double ng = f[(c * 19 + q) * N + i] * (double)gw(q);
+      u0 = u0 + ng * (double)cx(q);
+      u1 = u1 + ng * (double)cy(q);
+      u2 = u2 + ng * (double)cz(q);
+    }
+    rho[c * N + i] = r;
+    psi[c * N + i] = get_psi(r);
+    mom[(c * 3 + 0) * N + i] = u0;
+    mom[(c * 3 + 1) * N + i] = u1;
+    mom[(c * 3 + 2) * N + i] = u2;
+  }
+}
+
+__global__ void k_detmath(int fn, const double *x, double *y, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = x[i];
+  y[i] = fn == 0 ? det_exp(v) : fn == 1 ? lb3d_detmath::det_expm1(v) : det_tanh(v);
+}
+
+static inline unsigned grid_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace fp64
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+using namespace fp64;
+
+cudaError_t fp64_le_halo(const DevParams &P, const LEStep &S, const double *src, double *hlo,
+                         double *hhi, double *rlo, double *rhi, double *plo, double *phi,
+                         cudaStream_t st) {
+  int n = P.ny * P.nz;
+  if (P.nc == 2)
+    k_le_halo<2><<<grid_for(n, 128), 128, 0, st>>>(P, S, src, hlo, hhi, rlo, rhi, plo, phi);
+  else
+    k_le_halo<3><<<grid_for(n, 128), 128, 0, st>>>(P, S, src, hlo, hhi, rlo, rhi, plo, phi);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, double *rho,
+                        double *psi, double *mom, double *da, const double *db,
+                        const uint8_t *rock, const double *hlo, const double *hhi,
+                        cudaStream_t st) {
+  unsigned gr = grid_for(P.nsites, 256);
+  if (P.nc == 2) {
+    if (P.le)
+      k_stream<2, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi);
+    else
+      k_stream<2, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi);
+  } else {
+    k_stream<3, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_dipole(const DevParams &P, const double *rho, const double *da, double *db,
+                        cudaStream_t st) {
+  k_dipole<<<grid_for(P.nsites, 256), 256, 0, st>>>(P, rho, da, db);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_collide(const DevParams &P, const double *g, double *f, const double *rho,
+                         const double *psi, const double *mom, const double *db,
+                         const uint8_t *rock, const double *plo, const double *phi,
+                         cudaStream_t st) {
+  unsigned gr = grid_for(P.nsites, 256);
+  if (P.nc == 2) {
+    if (P.le)
+      k_collide<2, true><<<gr, 256, 0, st>>>(P, g, f, rho, psi, mom, db, rock, plo, phi);
+    else
+      k_collide<2, false><<<gr, 256, 0, st>>>(P, g, f, rho, psi, mom, db, rock, plo, phi);
+  } else {
+    k_collide<3, false><<<gr, 256, 0, st>>>(P, g, f, rho, psi, mom, db, rock, plo, phi);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_dump(const DevParams &P, int field, const double *f, const double *rho,
+                      const double *psi, const double *db, const uint8_t *rock, double *out,
+                      cudaStream_t st) {
+  unsigned gr = grid_for(P.nsites, 256);
+  if (P.nc == 2)
+    k_dump<2><<<gr, 256, 0, st>>>(P, field, f, rho, psi, db, rock, out);
+  else
+    k_dump<3><<<gr, 256, 0, st>>>(P, field, f, rho, psi, db, rock, out);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_moments(const DevParams &P, const double *f, double *rho, double *psi,
+                         double *mom, cudaStream_t st) {
+  unsigned gr = grid_for(P.nsites, 256);
+  if (P.nc == 2)
+    k_moments<2><<<gr, 256, 0, st>>>(P, f, rho, psi, mom);
+  else
+    k_moments<3><<<gr, 256, 0, st>>>(P, f, rho, psi, mom);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_detmath(int fn, const double *x, double *y, long long n, cudaStream_t st) {
+  k_detmath<<<grid_for(n, 256), 256, 0, st>>>(fn, x, y, n);
+  return cudaGetLastError();
+}
+
+}  // namespace lb3d

@@ -1,0 +1,32 @@
+// fp64_path.h -- host launchers of the FP64 drop-in kernels (fp64_path.cu).
+#ifndef LB3D_FP64_PATH_H
+#define LB3D_FP64_PATH_H
+
+#include "common.cuh"
+
+namespace lb3d {
+
+cudaError_t fp64_le_halo(const DevParams &P, const LEStep &S, const double *src, double *hlo,
+                         double *hhi, double *rlo, double *rhi, double *plo, double *phi,
+                         cudaStream_t st);
+cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, double *rho,
+                        double *psi, double *mom, double *da, const double *db,
+                        const uint8_t *rock, const double *hlo, const double *hhi,
+                        cudaStream_t st);
+cudaError_t fp64_dipole(const DevParams &P, const double *rho, const double *da, double *db,
+                        cudaStream_t st);
+cudaError_t fp64_collide(const DevParams &P, const double *g, double *f, const double *rho,
+                         const double *psi, const double *mom, const double *db,
+                         const uint8_t *rock, const double *plo, const double *phi,
+                         cudaStream_t st);
+// field: 0 od, 1 wd, 2 sur, 3 dir, 4 vel, 5 arr, 6 rock
+cudaError_t fp64_dump(const DevParams &P, int field, const double *f, const double *rho,
+                      const double *psi, const double *db, const uint8_t *rock, double *out,
+                      cudaStream_t st);
+cudaError_t fp64_moments(const DevParams &P, const double *f, double *rho, double *psi,
+                         double *mom, cudaStream_t st);
+cudaError_t fp64_detmath(int fn, const double *x, double *y, long long n, cudaStream_t st);
+
+}  // namespace lb3d
+
+#endif
