@@ -134,6 +134,30 @@ int lb3dc_time_loop(lb3dc_handle *h, int nsteps);
 /* Waits for all work of h; reports deferred kernel errors. */
 int lb3dc_sync(lb3dc_handle *h);
 
+/* ---- launch shape of the FP32 fused kernel ------------------------------ */
+/* Tile of the fused stream-collide kernel: tx x ty sites per CTA, zc planes
+ * per work item.  Supported (tx,ty): (32,8) (32,4) (16,16) (16,8) (64,4). */
+int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc);
+int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc);
+/* Times every supported shape on this lattice (on a saved copy of the
+ * state, which is restored afterwards) and keeps the fastest.  ms_out
+ * (optional, length >= 32) receives the measured ms per step of each tried
+ * shape in the order tried; returns the number tried in *ntried. */
+int lb3dc_autotune(lb3dc_handle *h, double *ms_out, int *ntried);
+
+/* ---- measurement ------------------------------------------------------ */
+/* The CUDA stream of h (a cudaStream_t), for callers that record their own
+ * events or order work against the handle. */
+void *lb3dc_stream(const lb3dc_handle *h);
+/* When enabled, every launch of the dominant kernel of a step (the fused
+ * stream-collide kernel of the FP32 path, the stream and collide kernels of
+ * the FP64 path) is bracketed by CUDA events on the handle's stream; the
+ * accumulated device time and launch count are read (synchronising) with
+ * lb3dc_kernel_stats and reset by lb3dc_set_profiling. */
+int lb3dc_set_profiling(lb3dc_handle *h, int enable);
+int lb3dc_kernel_stats(lb3dc_handle *h, double *ms_total, long long *launches,
+                       long long *all_launches);
+
 /* ---- Lees-Edwards bookkeeping (FP64 on the host) ---------------------- */
 int lb3dc_set_lees_edwards(lb3dc_handle *h, double shear_sum, double shear_u);
 int lb3dc_get_lees_edwards(const lb3dc_handle *h, double *shear_sum, double *shear_u);

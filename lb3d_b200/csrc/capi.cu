@@ -40,6 +40,7 @@ struct lb3dc_handle {
   double shear_u = 0.0, shear_tmp = 0.0, shear_sum = 0.0, lefrac = 0.0;
   int lelo = 0;
   bool pending_advection = false;  // FP32 path: advection deferred into collision
+  KernelTimer timer;
   std::string err;
   int errcode = 0;
 };
@@ -296,6 +297,7 @@ int lb3dc_destroy(lb3dc_handle *h) {
     if (b) cudaFree(b);
   if (h->rock) cudaFree(h->rock);
   fp32_free(h->s32);
+  h->timer.reset();
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return LB3DC_OK;
@@ -382,9 +384,7 @@ int lb3dc_download_state(lb3dc_handle *h, double *n, double *db, double *rho, do
     }
     CK(h, cudaStreamSynchronize(h->stream));
   } else {
-    rc = ensure_scratch(h, (long long)N * 19 * 8);
-    if (rc) return rc;
-    rc = fp32_download(h->P, h->p, h->s32, n, db, rho, mom, da, h->scratch, h->stream);
+    rc = fp32_download(h->P, h->p, h->s32, n, db, rho, mom, da, h->rock, h->stream);
     if (rc) return fail(h, rc, "FP32 download failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   return LB3DC_OK;
@@ -459,16 +459,20 @@ int lb3dc_bc_apply(lb3dc_handle *h, int stage) {
     if (h->le) {
       h->shear_u = h->shear_tmp * std::cos(h->p.shear_omega * (double)h->nt);
       le_neighbours(h);
-      if (h->p.precision == LB3DC_FP64)
+      if (h->p.precision == LB3DC_FP64) {
         CK(h, fp64_le_halo(h->P, le_step(h), h->f, h->hlo, h->hhi, nullptr, nullptr, nullptr,
                            nullptr, h->stream));
+        h->timer.launches += 1;
+      }
     }
     return LB3DC_OK;
   }
   if (stage == 8) {
-    if (h->le && h->p.precision == LB3DC_FP64)
+    if (h->le && h->p.precision == LB3DC_FP64) {
       CK(h, fp64_le_halo(h->P, le_step(h), h->g, nullptr, nullptr, h->rlo, h->rhi, h->plo,
                          h->phi, h->stream));
+      h->timer.launches += 1;
+    }
     return LB3DC_OK;
   }
   if (stage == 10) return LB3DC_OK;
@@ -479,8 +483,11 @@ int lb3dc_advection(lb3dc_handle *h) {
   int rc = need_loaded(h);
   if (rc) return rc;
   if (h->p.precision == LB3DC_FP64) {
+    h->timer.start(h->stream);
     CK(h, fp64_stream(h->P, h->f, h->g, h->rho, h->psi, h->mom, h->da, h->db, h->rock, h->hlo,
                       h->hhi, h->stream));
+    h->timer.stop(h->stream);
+    h->timer.launches += 1;
   } else {
     // The FP32 path streams inside its fused stream-collide kernel.
     h->pending_advection = true;
@@ -492,9 +499,15 @@ int lb3dc_collision(lb3dc_handle *h) {
   int rc = need_loaded(h);
   if (rc) return rc;
   if (h->p.precision == LB3DC_FP64) {
-    if (h->p.ncomp == 3) CK(h, fp64_dipole(h->P, h->rho, h->da, h->db, h->stream));
+    if (h->p.ncomp == 3) {
+      CK(h, fp64_dipole(h->P, h->rho, h->da, h->db, h->stream));
+      h->timer.launches += 1;
+    }
+    h->timer.start(h->stream);
     CK(h, fp64_collide(h->P, h->g, h->f, h->rho, h->psi, h->mom, h->db, h->rock, h->plo,
                        h->phi, h->stream));
+    h->timer.stop(h->stream);
+    h->timer.launches += 1;
   } else {
     if (!h->pending_advection)
       return fail(h, LB3DC_ESTATE, "collision without a preceding advection");
@@ -529,6 +542,54 @@ int lb3dc_sync(lb3dc_handle *h) {
   CK(h, cudaStreamSynchronize(h->stream));
   CK(h, cudaGetLastError());
   return LB3DC_OK;
+}
+
+void *lb3dc_stream(const lb3dc_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int lb3dc_set_profiling(lb3dc_handle *h, int enable) {
+  if (!h) return LB3DC_EINVAL;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  h->timer.reset();
+  h->timer.on = enable != 0;
+  h->s32.timer = &h->timer;
+  return LB3DC_OK;
+}
+
+int lb3dc_kernel_stats(lb3dc_handle *h, double *ms_total, long long *launches,
+                       long long *all_launches) {
+  if (!h) return LB3DC_EINVAL;
+  cudaSetDevice(h->device);
+  long long n = 0;
+  double ms = h->timer.collect(&n);
+  if (ms_total) *ms_total = ms;
+  if (launches) *launches = n;
+  if (all_launches) *all_launches = h->timer.launches;
+  return LB3DC_OK;
+}
+
+int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc) {
+  if (!h) return LB3DC_EINVAL;
+  if (h->p.precision != LB3DC_FP32_DEV) return fail(h, LB3DC_ENOTSUP, "launch shape applies to the FP32 path");
+  cudaSetDevice(h->device);
+  int rc = fp32_set_shape(h->P, h->s32, FusedShape{tx, ty, zc}, h->stream);
+  return rc ? fail(h, rc, "unsupported launch shape %dx%dx%d", tx, ty, zc) : LB3DC_OK;
+}
+
+int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc) {
+  if (!h) return LB3DC_EINVAL;
+  if (tx) *tx = h->s32.tx;
+  if (ty) *ty = h->s32.ty;
+  if (zc) *zc = h->s32.zc;
+  return LB3DC_OK;
+}
+
+int lb3dc_autotune(lb3dc_handle *h, double *ms_out, int *ntried) {
+  int rc = need_loaded(h);
+  if (rc) return rc;
+  if (h->p.precision != LB3DC_FP32_DEV) return fail(h, LB3DC_ENOTSUP, "autotune applies to the FP32 path");
+  rc = fp32_autotune(h->P, h->s32, h->rock, ms_out, ntried, h->stream);
+  return rc ? fail(h, rc, "autotune failed: %s", cudaGetErrorString(cudaGetLastError())) : LB3DC_OK;
 }
 
 int lb3dc_set_lees_edwards(lb3dc_handle *h, double shear_sum, double shear_u) {
@@ -600,7 +661,7 @@ int lb3dc_dump(lb3dc_handle *h, const char *field, double *out) {
     if (rc) return rc;
     CK(h, fp64_dump(h->P, fid, h->f, h->rho, h->psi, h->db, h->rock, h->scratch, h->stream));
   } else {
-    rc = ensure_scratch(h, N * 19 * 8);
+    rc = ensure_scratch(h, N * vps * 8);
     if (rc) return rc;
     rc = fp32_dump(h->P, h->s32, fid, h->rock, h->scratch, h->stream);
     if (rc) return fail(h, rc, "FP32 dump failed: %s", cudaGetErrorString(cudaGetLastError()));

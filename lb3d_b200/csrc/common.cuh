@@ -3,6 +3,7 @@
 #define LB3D_COMMON_CUH
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/lb3dc.h"
@@ -53,6 +54,41 @@ struct LEStep {
   double shear_u;
   double lefrac;
   int eoff;  // z offset of the bottom halo source: lelo (>= 0) or lelo-1
+};
+
+// Optional CUDA-event bracketing of the dominant kernel launches.
+struct KernelTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;  // pairs: start, stop
+  long long launches = 0;       // all kernel launches issued by the handle
+  void start(cudaStream_t st) {
+    if (!on) return;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+    ev.push_back(a);
+    ev.push_back(b);
+  }
+  void stop(cudaStream_t st) {
+    if (on && !ev.empty()) cudaEventRecord(ev.back(), st);
+  }
+  double collect(long long *n) {
+    double ms = 0;
+    for (size_t i = 0; i + 1 < ev.size(); i += 2) {
+      float t = 0;
+      cudaEventSynchronize(ev[i + 1]);
+      cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      ms += t;
+    }
+    if (n) *n = (long long)ev.size() / 2;
+    return ms;
+  }
+  void reset() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    ev.clear();
+    launches = 0;
+  }
 };
 
 LB3D_HDI int wrap(int v, int n) {

@@ -1,36 +1,960 @@
-// fp32_path.cu -- the FP32 deviation-storage path (LB3DC_FP32_DEV).
+// fp32_path.cu -- FP32 deviation storage, one fused stream-collide pass.
+//
+// Populations are stored as FP32 deviations delta_{c,i} = n_{c,i} - w_i rho0
+// from the rest state (w_i = 1/36 moving, 1/3 rest), so the stored values
+// and the moment sums carry the small variations at full FP32 relative
+// precision.  One kernel launch advances a step: each CTA owns a TX x TY
+// column tile and a range of z planes and marches in z with three stages
+// per plane, keeping every intermediate field on chip:
+//
+//   A(k)   post-stream moments on the tile plus a halo of H sites
+//          (H = 2 ternary, 1 binary): pull 19*nc deviations, densities,
+//          psi deviations dpsi = psi(rho) - psi(rho0) = -e^{-rho0}
+//          expm1(-drho), and (ternary) the advected dipole flux da using the
+//          previous dipoles staged in shared memory.
+//   B(k-1) (ternary) dipole relaxation on the tile plus a one-site halo
+//          from the A ring (code/lb3d_collision.F90:296-403).
+//   C(k-H) Shan-Chen force from the on-chip psi/dipole rings, body force,
+//          the pull of the own site's populations (an L2 hit: the same
+//          values were pulled by stage A two planes earlier), the
+//          equilibrium of code/lb3d_bdist.F90:301-370 in deviation form
+//          and the BGK update, written to the other buffer.
+//
+// HBM traffic per site and step is therefore one read and one write of the
+// 19*nc deviations (plus the dipoles and a rock byte), against ~800 B for a
+// three-kernel split.  Nothing in the path is a dense contraction, so there
+// are no tensor cores; the roofline is HBM bandwidth.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "fp32_path.h"
+#include "reduce.h"
+#include "fp64_path.h"
 
 namespace lb3d {
+namespace f32 {
 
+constexpr float W1 = 1.0f / 36.0f;
+constexpr float W0 = 1.0f / 3.0f;
+LB3D_HDI constexpr float wq(int q) { return q == 18 ? W0 : W1; }
+
+__device__ __forceinline__ int pmod(int v, int n) {
+  int r = v % n;
+  return r < 0 ? r + n : r;
+}
+
+// Langevin function L(x) = coth x - 1/x, accurate in FP32 for small x.
+__device__ __forceinline__ float langevin(float x) {
+  if (x < 0.3f) {
+    float x2 = x * x;
+    return x * (1.0f / 3.0f + x2 * (-1.0f / 45.0f + x2 * (2.0f / 945.0f + x2 * (-1.0f / 4725.0f))));
+  }
+  float t = tanhf(x);
+  return 1.0f / t - 1.0f / x;
+}
+
+// Equilibrium deviation for one component: out_i = rho*(E_i(v) - w_i) + drho*w_i
+// with E of bdist = 2 (code/lb3d_bdist.F90:301-370), then the BGK update
+// d_i <- d_i + omega (deq_i - d_i).
+__device__ __forceinline__ void bgk_update(float d[19], float rho, float drho, float vx, float vy,
+                                           float vz, float omega) {
+  const float tx = 3.0f * vx, ty = 3.0f * vy, tz = 3.0f * vz;
+  const float uke = 0.5f * (tx * vx + ty * vy + tz * vz);
+  const float a = -uke;          // even part minus w
+  const float b = 1.0f - uke;    // odd linear coefficient
+  const float rw = rho * W1;
+  const float base = drho * W1;
+#define LB3D_PAIR32(CD, I, J)                                             \
+  {                                                                       \
+    const float e = (CD);                                                 \
+    const float e2 = e * e;                                               \
+    const float ev = rw * fmaf(0.5f, e2, a) + base;                       \
+    const float od = rw * e * fmaf(e2, 1.0f / 6.0f, b);                   \
+    d[I] = fmaf(omega, (ev + od) - d[I], d[I]);                           \
+    d[J] = fmaf(omega, (ev - od) - d[J], d[J]);                           \
+  }
+  LB3D_PAIR32(tx, 0, 1)
+  LB3D_PAIR32(ty, 2, 3)
+  LB3D_PAIR32(tz, 4, 5)
+  LB3D_PAIR32(tx + ty, 6, 11)
+  LB3D_PAIR32(tx - ty, 7, 10)
+  LB3D_PAIR32(tx + tz, 8, 13)
+  LB3D_PAIR32(tx - tz, 9, 12)
+  LB3D_PAIR32(ty + tz, 14, 17)
+  LB3D_PAIR32(ty - tz, 15, 16)
+#undef LB3D_PAIR32
+  const float deq0 = rho * W0 * a + drho * W0;
+  d[18] = fmaf(omega, deq0 - d[18], d[18]);
+}
+
+// Site offsets (32-bit, relative to the lattice base) of the -1, 0, +1
+// neighbours along each axis, with the periodic wrap applied once.
+struct Nbr {
+  int cx[3], ry[3], rz[3];
+};
+
+__device__ __forceinline__ void make_nbr(Nbr &n, int gx, int gy, int gz, int nx, int ny, int nz) {
+  const int pl = nx * ny;
+  n.cx[0] = gx == 0 ? nx - 1 : gx - 1;
+  n.cx[1] = gx;
+  n.cx[2] = gx == nx - 1 ? 0 : gx + 1;
+  n.ry[0] = (gy == 0 ? ny - 1 : gy - 1) * nx;
+  n.ry[1] = gy * nx;
+  n.ry[2] = (gy == ny - 1 ? 0 : gy + 1) * nx;
+  n.rz[0] = (gz == 0 ? nz - 1 : gz - 1) * pl;
+  n.rz[1] = gz * pl;
+  n.rz[2] = (gz == nz - 1 ? 0 : gz + 1) * pl;
+}
+// site offset of x + s*c_q (s = +1 neighbour, s = -1 upstream)
+template <int Q, int SGN>
+__device__ __forceinline__ int noff(const Nbr &n) {
+  return n.cx[1 + SGN * cx(Q)] + n.ry[1 + SGN * cy(Q)] + n.rz[1 + SGN * cz(Q)];
+}
+
+// Pulls the post-stream deviations of component C of one site (with
+// half-way bounce-back when ROCK): d[q] = delta*(x - c_q, q), or
+// delta*(x, bounce(q)) when x - c_q is rock (code/lb3d_bc_bounce.F90:53-90
+// with code/lb3d_advection.F90:109-151).  F points at component 0 of the
+// lattice; the component stride is 19*S.
+template <bool ROCK>
+__device__ __forceinline__ void pull_comp(const float *__restrict__ F, int S, int c, const Nbr &n,
+                                          int self, const uint8_t *__restrict__ rk, float d[19]) {
+  const float *fc = F + c * 19 * S;
+  d[18] = __ldg(fc + 18 * S + self);
+#define LB3D_PULL(Q)                                                     \
+  {                                                                      \
+    const int up = noff<Q, -1>(n);                                       \
+    bool uf = true;                                                      \
+    if (ROCK) uf = __ldg(rk + up) == 0;                                  \
+    d[Q] = __ldg(fc + (uf ? Q * S + up : bounce(Q) * S + self));         \
+  }
+  LB3D_PULL(0) LB3D_PULL(1) LB3D_PULL(2) LB3D_PULL(3) LB3D_PULL(4) LB3D_PULL(5)
+  LB3D_PULL(6) LB3D_PULL(7) LB3D_PULL(8) LB3D_PULL(9) LB3D_PULL(10) LB3D_PULL(11)
+  LB3D_PULL(12) LB3D_PULL(13) LB3D_PULL(14) LB3D_PULL(15) LB3D_PULL(16) LB3D_PULL(17)
+#undef LB3D_PULL
+}
+
+// ---------------------------------------------------------------------------
+// The fused kernel.  Grid: persistent CTAs over a tile list.  Populations
+// of lattice L live at f[(c*19+q)*S + L.base + site]; offsets are 32-bit,
+// which bounds the packed capacity at 19*nc*S < 2^31.
+// ---------------------------------------------------------------------------
+template <int NC, int TX, int TY, bool ROCK, bool BODY>
+__global__ void __launch_bounds__(TX *TY, 1)
+    k_fused(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
+            float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, int S) {
+  constexpr int NT = TX * TY;
+  constexpr int H = (NC == 3) ? 2 : 1;  // halo of the moment stage
+  constexpr int AW = TX + 2 * H, AH = TY + 2 * H, AN = AW * AH;
+  constexpr int AF = (NC == 3) ? 8 : 2;  // fields per A entry
+  constexpr int AR = (NC == 3) ? 4 : 3;  // A ring depth
+  constexpr int BW = TX + 2, BH = TY + 2, BN = BW * BH;
+  constexpr int DW = TX + 6, DH = TY + 6, DN = DW * DH;
+  // A fields (ternary): 0 rho_b - rho_r, 1 drho_s, 2..4 da, 5 dpsi_r,
+  // 6 dpsi_b, 7 dpsi_s.   Binary: 0 dpsi_r, 1 dpsi_b.
+  extern __shared__ float smem[];
+  float *ringA = smem;                                  // [AR][AF][AN]
+  float *ringB = ringA + AR * AF * AN;                  // [3][3][BN]   (ternary)
+  float *ringD = ringB + ((NC == 3) ? 3 * 3 * BN : 0);  // [3][3][DN]   (ternary)
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    const LatDesc &Lg = lats[T.lat];
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    const int base = (int)Lg.base;
+    const int par = Lg.parity;
+    const float *__restrict__ F = (par ? f1 : f0) + base;
+    float *__restrict__ Fo = (par ? f0 : f1) + base;
+    const float *__restrict__ DBi = (NC == 3) ? (par ? db1 : db0) + base : nullptr;
+    float *__restrict__ DBo = (NC == 3) ? (par ? db0 : db1) + base : nullptr;
+    const uint8_t *__restrict__ RK = rock + base;
+    const float rho0 = Lg.rho0, em0 = Lg.em0, psi0 = Lg.psi0;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const int zfirst = z0 - H;
+    const int niter = zc + 2 * H;
+
+    // ternary: previous dipoles of one plane (with a 3-site xy halo) into
+    // the D ring; plane zfirst - 1 + j goes to slot j % 3.
+    auto load_db_plane = [&](int j) {
+      const int gz = pmod(zfirst - 1 + j, nz);
+      float *dst = ringD + (j % 3) * 3 * DN;
+      for (int s = tid; s < DN; s += NT) {
+        const int gx = pmod(x0 - 3 + s % DW, nx), gy = pmod(y0 - 3 + s / DW, ny);
+        const int i = gx + nx * (gy + ny * gz);
+        dst[s] = __ldg(DBi + i);
+        dst[DN + s] = __ldg(DBi + S + i);
+        dst[2 * DN + s] = __ldg(DBi + 2 * S + i);
+      }
+    };
+    if (NC == 3) {
+      load_db_plane(0);
+      load_db_plane(1);
+    }
+
+    for (int it = 0; it < niter; ++it) {
+      const int zA = zfirst + it;
+      if (NC == 3) load_db_plane(it + 2);
+      __syncthreads();
+      // ---------------- stage A: post-stream moments on the haloed tile ----
+      {
+        float *slot = ringA + (it % AR) * AF * AN;
+        const int gz = pmod(zA, nz);
+        for (int s = tid; s < AN; s += NT) {
+          const int ax = s % AW, ay = s / AW;
+          const int gx = pmod(x0 - H + ax, nx), gy = pmod(y0 - H + ay, ny);
+          Nbr nb;
+          make_nbr(nb, gx, gy, gz, nx, ny, nz);
+          const int self = noff<18, 1>(nb);
+          float dr[NC];
+          float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            float d[19];
+            pull_comp<ROCK>(F, S, c, nb, self, RK, d);
+            float acc = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) acc += (float)gw(q) * d[q];
+            dr[c] = acc;
+            if (NC == 3 && c == 2) {
+              // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
+              // (code/lb3d_advection.F90:137-148)
+              const int dx = ax + 1, dy = ay + 1;  // A-local -> D-local
+#pragma unroll
+              for (int q = 0; q < 19; ++q) {
+                const float *Dp = ringD + ((it + 1 - cz(q)) % 3) * 3 * DN;
+                const int ds = (dx - cx(q)) + DW * (dy - cy(q));
+                const float ng = (float)gw(q) * (d[q] + wq(q) * rho0);
+                a0 = fmaf(ng, Dp[ds], a0);
+                a1 = fmaf(ng, Dp[DN + ds], a1);
+                a2 = fmaf(ng, Dp[2 * DN + ds], a2);
+              }
+            }
+          }
+          if (NC == 3) {
+            slot[0 * AN + s] = dr[1] - dr[0];
+            slot[1 * AN + s] = dr[NC - 1];
+            slot[2 * AN + s] = a0;
+            slot[3 * AN + s] = a1;
+            slot[4 * AN + s] = a2;
+            slot[5 * AN + s] = -em0 * expm1f(-dr[0]);
+            slot[6 * AN + s] = -em0 * expm1f(-dr[1]);
+            slot[7 * AN + s] = -em0 * expm1f(-dr[NC - 1]);
+          } else {
+            slot[0 * AN + s] = -em0 * expm1f(-dr[0]);
+            slot[1 * AN + s] = -em0 * expm1f(-dr[1]);
+          }
+        }
+      }
+      __syncthreads();
+      // ---------------- stage B (ternary): dipole relaxation ----------------
+      if (NC == 3 && it >= 2) {
+        float *slotB = ringB + (it % 3) * 3 * BN;
+        const int zB = zA - 1;
+        const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
+        const float *Ac = ringA + ((it - 1) % AR) * AF * AN;
+        for (int s = tid; s < BN; s += NT) {
+          const int bx = s % BW, by = s / BW;
+          const int as = (bx + 1) + AW * (by + 1);
+          float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
+          float hs0 = Ac[2 * AN + as], hs1 = Ac[3 * AN + as], hs2 = Ac[4 * AN + as];
+          const float isN = 1.0f / fmaxf(rho0 + Ac[1 * AN + as], 1.0e-4f);
+          const float st0 = hs0 * isN, st1 = hs1 * isN, st2 = hs2 * isN;
+#pragma unroll
+          for (int q = 0; q < 18; ++q) {
+            const float *Ap = ringA + ((it - 1 + cz(q)) % AR) * AF * AN;
+            const int an = as + cx(q) + AW * cy(q);
+            const float g = (float)gw(q);
+            const float hcm = -sgn * Ap[an] * g;  // field 0 = rho_b - rho_r
+            const float p0 = Ap[2 * AN + an], p1 = Ap[3 * AN + an], p2 = Ap[4 * AN + an];
+            const float dot2 = 2.0f * (cx(q) * p0 + cy(q) * p1 + cz(q) * p2);
+            hc0 += hcm * cx(q);
+            hc1 += hcm * cy(q);
+            hc2 += hcm * cz(q);
+            hs0 += (p0 - cx(q) * dot2) * g;
+            hs1 += (p1 - cy(q) * dot2) * g;
+            hs2 += (p2 - cz(q) * dot2) * g;
+          }
+          const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
+          const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
+          const float hm = Lg.beta * hn;
+          // d_eq = d0 L(beta|h|) h/|h| with the Langevin function L; the
+          // reference's small-field branch beta h / 3 (h_m <= 0.01) is L's
+          // first-order term.
+          float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
+          const float od = Lg.omega_d, om1 = 1.0f - od;
+          const float n0 = od * fac * h0 + om1 * st0;
+          const float n1 = od * fac * h1 + om1 * st1;
+          const float n2 = od * fac * h2 + om1 * st2;
+          slotB[s] = n0;
+          slotB[BN + s] = n1;
+          slotB[2 * BN + s] = n2;
+          if (bx >= 1 && bx <= TX && by >= 1 && by <= TY && zB >= z0 && zB < z0 + zc) {
+            const int gx = x0 + bx - 1, gy = y0 + by - 1;
+            if (gx < nx && gy < ny) {
+              const int i = gx + nx * (gy + ny * pmod(zB, nz));
+              DBo[i] = n0;
+              DBo[S + i] = n1;
+              DBo[2 * S + i] = n2;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      // ---------------- stage C: force + BGK on the tile ---------------------
+      const int itC = it - H;  // A iteration of plane zC
+      const int zC = zA - H;
+      if (zC >= z0 && zC < z0 + zc) {
+        const int gx = x0 + tx, gy = y0 + ty;
+        if (gx < nx && gy < ny) {
+          const int gz = pmod(zC, nz);
+          Nbr nb;
+          make_nbr(nb, gx, gy, gz, nx, ny, nz);
+          const int self = noff<18, 1>(nb);
+          bool own_rock = false;
+          if (ROCK) own_rock = __ldg(RK + self) != 0;
+          if (!own_rock) {
+            const int as = (tx + H) + AW * (ty + H);
+            const float *A0 = ringA + (itC % AR) * AF * AN;
+            float Fx[NC][3];
+            float psi_own[NC];
+            if (NC == 3) {
+              // ---- ternary Shan-Chen force, code/lb3d_force_shanchen.F90:215-330
+              const int itB = itC + 1;  // B computed plane zC at iteration itC + 1
+              const int bs = (tx + 1) + BW * (ty + 1);
+              const float *B0 = ringB + (itB % 3) * 3 * BN;
+              const float d0x = B0[bs], d1x = B0[BN + bs], d2x = B0[2 * BN + bs];
+              float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fcs[3] = {0, 0, 0}, fsc[3] = {0, 0, 0},
+                    fss[3] = {0, 0, 0};
+#pragma unroll
+              for (int q = 0; q < 18; ++q) {
+                const float *Ap = ringA + ((itC + cz(q)) % AR) * AF * AN;
+                const float *Bp = ringB + ((itB + cz(q)) % 3) * 3 * BN;
+                const int an = as + cx(q) + AW * cy(q);
+                const int bn = bs + cx(q) + BW * cy(q);
+                const float g = (float)gw(q);
+                const float c[3] = {(float)cx(q), (float)cy(q), (float)cz(q)};
+                const float pr = Ap[5 * AN + an], pb = Ap[6 * AN + an];
+                const float ps = psi0 + Ap[7 * AN + an];
+                const float a[3] = {Bp[bn] * ps, Bp[BN + bn] * ps, Bp[2 * BN + bn] * ps};
+                const float ddc = a[0] * c[0] + a[1] * c[1] + a[2] * c[2];
+                const float dic = d0x * c[0] + d1x * c[1] + d2x * c[2];
+                const float did = a[0] * d0x + a[1] * d1x + a[2] * d2x;
+                const float gcs = (pb - pr) * g;
+                const float dx[3] = {d0x, d1x, d2x};
+                const float s8 = 8.0f * g;
+                const float coef = did - 2.0f * dic * ddc;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                  if (c[k] != 0.0f) {
+                    frb[k] = fmaf(pb * g, c[k], frb[k]);
+                    fbr[k] = fmaf(pr * g, c[k], fbr[k]);
+                  }
+                  fcs[k] += (a[k] - 2.0f * ddc * c[k]) * g;
+                  fsc[k] = fmaf(gcs, dx[k] - 2.0f * dic * c[k], fsc[k]);
+                  fss[k] = fmaf(s8, coef * c[k] + a[k] * dic + ddc * dx[k], fss[k]);
+                }
+              }
+              psi_own[0] = psi0 + A0[5 * AN + as];
+              psi_own[1] = psi0 + A0[6 * AN + as];
+              psi_own[NC - 1] = psi0 + A0[7 * AN + as];
+#pragma unroll
+              for (int k = 0; k < 3; ++k) {
+                const float cs = -2.0f * Lg.g_bs * fcs[k];
+                Fx[1][k] = (-Lg.g_br * fbr[k] + cs) * psi_own[1];
+                Fx[0][k] = (-Lg.g_br * frb[k] - cs) * psi_own[0];
+                Fx[NC - 1][k] = (2.0f * Lg.g_bs * fsc[k] - Lg.g_ss * fss[k]) * psi_own[NC - 1];
+              }
+            } else {
+              // ---- binary Shan-Chen force with walls, :127-210
+              float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
+#pragma unroll
+              for (int q = 0; q < 18; ++q) {
+                const float *Ap = ringA + ((itC + cz(q)) % AR) * AF * AN;
+                const int an = as + cx(q) + AW * cy(q);
+                const float g = (float)gw(q);
+                const float c[3] = {(float)cx(q), (float)cy(q), (float)cz(q)};
+                bool nrock = false;
+                if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
+                if (nrock) {
+                  // a rock neighbour contributes psi(0 + rock colour) to the
+                  // wall sums; the fluid sums run over fluid neighbours only,
+                  // so their psi(rho0) share no longer cancels and is removed.
+#pragma unroll
+                  for (int k = 0; k < 3; ++k)
+                    if (c[k] != 0.0f) {
+                      fwb[k] = fmaf(Lg.psiw_b * g, c[k], fwb[k]);
+                      fwr[k] = fmaf(Lg.psiw_r * g, c[k], fwr[k]);
+                      frb[k] = fmaf(-psi0 * g, c[k], frb[k]);
+                      fbr[k] = fmaf(-psi0 * g, c[k], fbr[k]);
+                    }
+                } else {
+                  const float pr = Ap[0 * AN + an], pb = Ap[1 * AN + an];
+#pragma unroll
+                  for (int k = 0; k < 3; ++k)
+                    if (c[k] != 0.0f) {
+                      frb[k] = fmaf(pb * g, c[k], frb[k]);
+                      fbr[k] = fmaf(pr * g, c[k], fbr[k]);
+                    }
+                }
+              }
+              psi_own[0] = psi0 + A0[0 * AN + as];
+              psi_own[1] = psi0 + A0[1 * AN + as];
+#pragma unroll
+              for (int k = 0; k < 3; ++k) {
+                Fx[1][k] = (-Lg.g_br * fbr[k] + Lg.wall_b * fwb[k]) * psi_own[1];
+                Fx[0][k] = (-Lg.g_br * frb[k] + Lg.wall_r * fwr[k]) * psi_own[0];
+              }
+            }
+            // ---- pass 1: moments of the own post-stream populations (the
+            // pulls hit L2: stage A fetched them H planes earlier)
+            float dr[NC], j[NC][3];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              float d[19];
+              pull_comp<ROCK>(F, S, c, nb, self, RK, d);
+              float r = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f;
+#pragma unroll
+              for (int q = 0; q < 19; ++q) {
+                const float ng = (float)gw(q) * d[q];
+                r += ng;
+                if (cx(q)) j0 += cx(q) * ng;
+                if (cy(q)) j1 += cy(q) * ng;
+                if (cz(q)) j2 += cz(q) * ng;
+              }
+              dr[c] = r;
+              j[c][0] = j0;
+              j[c][1] = j1;
+              j[c][2] = j2;
+            }
+            float rho[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) rho[c] = rho0 + dr[c];
+            if (BODY) {
+              const int x1 = gx + 1, y1 = gy + 1, z1 = gz + 1;
+              bool on;
+              if (Lg.inv_fluid == 9)
+                on = (z1 == 1) || (z1 == nz);
+              else if (Lg.inv_fluid == 20 || Lg.inv_fluid == 21)
+                on = z1 == 1;
+              else
+                on = z1 >= Lg.amin_z && z1 <= Lg.amax_z && x1 >= Lg.amin_x && x1 <= Lg.amax_x &&
+                     y1 >= Lg.amin_y && y1 <= Lg.amax_y;
+              if (on) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                  const float m = Lg.amass[c] * rho[c];
+                  Fx[c][0] = fmaf(m, Lg.g_accn_x, Fx[c][0]);
+                  Fx[c][1] = fmaf(m, Lg.g_accn_y, Fx[c][1]);
+                  Fx[c][2] = fmaf(m, Lg.g_accn, Fx[c][2]);
+                }
+              }
+            }
+            // common velocity u~ (code/lb3d_collision.F90:560-587)
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f, rt = 0.f;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const float am = Lg.amass[c] * Lg.omega[c];
+              p0 = fmaf(am, j[c][0], p0);
+              p1 = fmaf(am, j[c][1], p1);
+              p2 = fmaf(am, j[c][2], p2);
+              rt = fmaf(am, rho[c], rt);
+            }
+            const float irt = 1.0f / fmaxf(rt, 1.0e-8f);
+            const float u0 = p0 * irt, u1 = p1 * irt, u2 = p2 * irt;
+            // ---- pass 2: reload (L1), relax, store
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              // du = tau F / (amass max(rho, 1e-8))  (:523-556)
+              const float k = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
+              float d[19];
+              pull_comp<ROCK>(F, S, c, nb, self, RK, d);
+              bgk_update(d, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
+                         fmaf(k, Fx[c][2], u2), Lg.omega[c]);
+              float *fo = Fo + c * 19 * S + self;
+#pragma unroll
+              for (int q = 0; q < 19; ++q) fo[q * S] = d[q];
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void k_flip(LatDesc *lats, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && (lats[i].flags & LAT_ACTIVE)) lats[i].parity ^= 1;
+}
+
+// FP32 state -> FP64 populations n = delta + w rho0 (dumps, reductions).
+__global__ void k_to_fp64(const float *__restrict__ f, double *__restrict__ n, long long S,
+                          long long base, long long N, int nc, double rho0) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int c = 0; c < nc; ++c)
+    for (int q = 0; q < 19; ++q)
+      n[((long long)c * 19 + q) * N + i] =
+          (double)f[((long long)c * 19 + q) * S + base + i] + (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+}
+
+}  // namespace f32
+
+using namespace f32;
+
+// ---------------------------------------------------------------------------
+// launch table
+// ---------------------------------------------------------------------------
+size_t fp32_fused_smem(int nc, const FusedShape &sh) {
+  const int H = nc == 3 ? 2 : 1;
+  const size_t AN = (size_t)(sh.tx + 2 * H) * (sh.ty + 2 * H);
+  const size_t BN = (size_t)(sh.tx + 2) * (sh.ty + 2);
+  const size_t DN = (size_t)(sh.tx + 6) * (sh.ty + 6);
+  if (nc == 3) return 4 * (4 * 8 * AN + 3 * 3 * BN + 3 * 3 * DN);
+  return 4 * (3 * 2 * AN);
+}
+
+template <int NC, int TX, int TY, bool ROCK, bool BODY>
+static const void *fused_ptr() {
+  return (const void *)k_fused<NC, TX, TY, ROCK, BODY>;
+}
+
+static const void *fused_fn(int nc, bool rock, bool body, const FusedShape &sh) {
+#define LB3D_SHAPES(NC, R, B)                                                  \
+  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B>();          \
+  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B>();          \
+  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B>();        \
+  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B>();          \
+  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B>();
+  if (nc == 3) {
+    if (body) { LB3D_SHAPES(3, false, true) } else { LB3D_SHAPES(3, false, false) }
+  } else {
+    if (rock) {
+      if (body) { LB3D_SHAPES(2, true, true) } else { LB3D_SHAPES(2, true, false) }
+    } else {
+      if (body) { LB3D_SHAPES(2, false, true) } else { LB3D_SHAPES(2, false, false) }
+    }
+  }
+#undef LB3D_SHAPES
+  return nullptr;
+}
+
+int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh) {
+  const void *fn = fused_fn(nc, rock, body, sh);
+  if (!fn) return 0;
+  size_t smem = fp32_fused_smem(nc, sh);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, sh.tx * sh.ty, smem) != cudaSuccess) return 0;
+  return n;
+}
+
+cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
+                              const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
+                              float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
+                              long long S64, cudaStream_t st) {
+  const void *fn = fused_fn(nc, rock, body, sh);
+  if (S64 * 19 * nc >= (1LL << 31)) return cudaErrorInvalidValue;
+  int S = (int)S64;
+  if (!fn) return cudaErrorInvalidConfiguration;
+  size_t smem = fp32_fused_smem(nc, sh);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&f0, (void *)&f1,
+                  (void *)&db0, (void *)&db1, (void *)&rockp, (void *)&S};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
+}
+
+cudaError_t fp32_flip_parity(LatDesc *d_lat, int nlat, cudaStream_t st) {
+  k_flip<<<(nlat + 127) / 128, 128, 0, st>>>(d_lat, nlat);
+  return cudaGetLastError();
+}
+
+void fp32_tiles_for(const LatDesc &L, int lat_id, const FusedShape &sh, std::vector<Tile> &out) {
+  const int zc = std::min(sh.zc, L.nz);
+  for (int z0 = 0; z0 < L.nz; z0 += zc)
+    for (int y0 = 0; y0 < L.ny; y0 += sh.ty)
+      for (int x0 = 0; x0 < L.nx; x0 += sh.tx) {
+        Tile t;
+        t.lat = lat_id;
+        t.x0 = (short)x0;
+        t.y0 = (short)y0;
+        t.z0 = (short)z0;
+        t.zc = (short)std::min(zc, L.nz - z0);
+        out.push_back(t);
+      }
+}
+
+LatDesc fp32_make_desc(const DevParams &P, double rho0, long long base, bool rock) {
+  LatDesc L{};
+  L.nx = P.nx;
+  L.ny = P.ny;
+  L.nz = P.nz;
+  L.nc = P.nc;
+  L.base = base;
+  L.parity = 0;
+  for (int c = 0; c < 3; ++c) {
+    L.omega[c] = (float)P.omega[c];
+    L.tau[c] = (float)P.tau[c];
+    L.amass[c] = (float)P.amass[c];
+  }
+  L.g_br = (float)P.g_br;
+  L.g_bs = (float)P.g_bs;
+  L.g_ss = (float)P.g_ss;
+  L.wall_r = (float)(-P.g_wr * P.tau_wr / P.tau[0]);
+  L.wall_b = (float)(-P.g_wb * P.tau_wb / P.tau[1]);
+  L.psiw_r = (float)(1.0 - std::exp(-P.rc_r));
+  L.psiw_b = (float)(1.0 - std::exp(-P.rc_b));
+  L.beta = (float)P.beta;
+  L.d0 = (float)P.d_0;
+  L.omega_d = (float)P.omega_d;
+  L.g_accn = (float)P.g_accn;
+  L.g_accn_x = (float)P.g_accn_x;
+  L.g_accn_y = (float)P.g_accn_y;
+  L.amin_x = P.g_accn_min_x;
+  L.amax_x = P.g_accn_max_x;
+  L.amin_y = P.g_accn_min_y;
+  L.amax_y = P.g_accn_max_y;
+  L.amin_z = P.g_accn_min;
+  L.amax_z = P.g_accn_max;
+  L.inv_fluid = P.inv_fluid;
+  L.rho0 = (float)rho0;
+  L.em0 = (float)std::exp(-rho0);
+  L.psi0 = (float)(1.0 - std::exp(-rho0));
+  bool body = (P.g_accn != 0.0 || P.g_accn_x != 0.0 || P.g_accn_y != 0.0);
+  L.flags = LAT_ACTIVE | (rock ? LAT_ROCK : 0) | (body ? LAT_BODY : 0);
+  return L;
+}
+
+// ---------------------------------------------------------------------------
+// single-lattice handle
+// ---------------------------------------------------------------------------
 long long fp32_footprint(const lb3dc_params &p) {
   const long long N = (long long)p.nx * p.ny * p.nz;
-  return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0);
+  return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) + 4096;
 }
-int fp32_alloc(const DevParams &, const lb3dc_params &, Fp32State &, cudaStream_t) {
-  return LB3DC_ENOTSUP;
+
+static FusedShape default_shape(const DevParams &P) {
+  FusedShape sh{32, 8, 16};
+  if (P.nx < 32) sh = FusedShape{16, 16, 16};
+  if (P.nc == 2) sh.zc = 32;
+  return sh;
 }
-void fp32_free(Fp32State &) {}
-int fp32_upload(const DevParams &, const lb3dc_params &, Fp32State &, const double *,
-                const double *, const uint8_t *, cudaStream_t) {
-  return LB3DC_ENOTSUP;
+
+static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
+  std::vector<Tile> tiles;
+  fp32_tiles_for(s.lat, 0, sh, tiles);
+  if (s.d_tiles) cudaFree(s.d_tiles);
+  s.d_tiles = nullptr;
+  if (cudaMalloc(&s.d_tiles, tiles.size() * sizeof(Tile)) != cudaSuccess) return LB3DC_ENOMEM;
+  if (cudaMemcpyAsync(s.d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                      st) != cudaSuccess)
+    return LB3DC_ECUDA;
+  s.ntiles = (int)tiles.size();
+  s.tx = sh.tx;
+  s.ty = sh.ty;
+  s.zc = sh.zc;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  bool rock = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
+  int per = fp32_fused_ctas_per_sm(P.nc, rock, body, sh);
+  if (per < 1) return LB3DC_EINVAL;
+  s.grid = std::min(s.ntiles, per * nsm);
+  return LB3DC_OK;
 }
-int fp32_download(const DevParams &, const lb3dc_params &, Fp32State &, double *, double *,
-                  double *, double *, double *, double *, cudaStream_t) {
-  return LB3DC_ENOTSUP;
+
+int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
+  if (!fused_fn(P.nc, false, false, sh)) return LB3DC_EINVAL;
+  if (sh.zc < 1) return LB3DC_EINVAL;
+  return rebuild_tiles(P, s, sh, st);
 }
-int fp32_step(const DevParams &, Fp32State &, const uint8_t *, cudaStream_t) { return LB3DC_ENOTSUP; }
-int fp32_run(const DevParams &, Fp32State &, const uint8_t *, int, cudaStream_t) { return LB3DC_ENOTSUP; }
-int fp32_dump(const DevParams &, Fp32State &, int, const uint8_t *, double *, cudaStream_t) {
-  return LB3DC_ENOTSUP;
+
+std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
+  std::vector<FusedShape> out;
+  const int xy[5][2] = {{32, 8}, {32, 4}, {16, 16}, {16, 8}, {64, 4}};
+  const int zcs[3] = {8, 16, 32};
+  for (auto &t : xy) {
+    if (t[0] > 2 * P.nx && t[0] > 16) continue;
+    for (int zc : zcs) {
+      if (zc > P.nz && zc != 8) continue;
+      out.push_back(FusedShape{t[0], t[1], zc});
+    }
+  }
+  return out;
 }
-cudaError_t fp32_reduce_conservation(const DevParams &, Fp32State &, const uint8_t *, double *,
-                                     double *, double *, cudaStream_t) {
-  return cudaErrorNotSupported;
+
+// The project's autotuner: time each candidate shape with CUDA events on a
+// saved copy of the state, keep the fastest and restore the state.
+int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double *ms_out,
+                  int *ntried, cudaStream_t st) {
+  const size_t pop = (size_t)P.nc * 19 * s.S * sizeof(float);
+  const size_t dbs = P.nc == 3 ? 3 * (size_t)s.S * sizeof(float) : 0;
+  float *save = nullptr;
+  if (cudaMalloc(&save, pop + dbs) != cudaSuccess) return LB3DC_ENOMEM;
+  const int cur0 = s.lat.parity;
+  cudaMemcpyAsync(save, s.f[cur0], pop, cudaMemcpyDeviceToDevice, st);
+  if (dbs) cudaMemcpyAsync((char *)save + pop, s.db[cur0], dbs, cudaMemcpyDeviceToDevice, st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  FusedShape best{s.tx, s.ty, s.zc};
+  float best_ms = 1e30f;
+  KernelTimer *saved_timer = s.timer;
+  s.timer = nullptr;
+  int n = 0;
+  for (const FusedShape &sh : fp32_candidate_shapes(P)) {
+    if (rebuild_tiles(P, s, sh, st) != LB3DC_OK) continue;
+    if (fp32_run(P, s, rock, 2, st) != LB3DC_OK) continue;
+    cudaEventRecord(e0, st);
+    const int reps = 5;
+    if (fp32_run(P, s, rock, reps, st) != LB3DC_OK) continue;
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= reps;
+    if (ms_out && n < 32) ms_out[n] = ms;
+    ++n;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = sh;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // restore the state into the buffer the lattice now reads from
+  const int cur = s.lat.parity;
+  cudaMemcpyAsync(s.f[cur], save, pop, cudaMemcpyDeviceToDevice, st);
+  if (dbs) cudaMemcpyAsync(s.db[cur], (char *)save + pop, dbs, cudaMemcpyDeviceToDevice, st);
+  cudaStreamSynchronize(st);
+  cudaFree(save);
+  if (ntried) *ntried = n;
+  s.timer = saved_timer;
+  int rc = rebuild_tiles(P, s, best, st);
+  if (rc) return rc;
+  return cudaStreamSynchronize(st) == cudaSuccess ? LB3DC_OK : LB3DC_ECUDA;
 }
-cudaError_t fp32_sanity_counts(const DevParams &, Fp32State &, unsigned long long *,
-                               unsigned long long *, cudaStream_t) {
-  return cudaErrorNotSupported;
+
+int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStream_t st) {
+  const long long N = P.nsites;
+  s.S = N;
+  const size_t pop = (size_t)P.nc * 19 * N * sizeof(float);
+  for (int b = 0; b < 2; ++b) {
+    if (cudaMalloc(&s.f[b], pop) != cudaSuccess) return LB3DC_ENOMEM;
+    s.bytes += pop;
+    cudaMemsetAsync(s.f[b], 0, pop, st);
+    if (P.nc == 3) {
+      if (cudaMalloc(&s.db[b], 3 * N * sizeof(float)) != cudaSuccess) return LB3DC_ENOMEM;
+      s.bytes += 3 * N * sizeof(float);
+      cudaMemsetAsync(s.db[b], 0, 3 * N * sizeof(float), st);
+    }
+  }
+  if (cudaMalloc(&s.d_lat, sizeof(LatDesc)) != cudaSuccess) return LB3DC_ENOMEM;
+  s.lat = fp32_make_desc(P, p.rho0 > 0 ? p.rho0 : 0.7, 0, false);
+  return rebuild_tiles(P, s, default_shape(P), st);
+}
+
+void fp32_free(Fp32State &s) {
+  for (int b = 0; b < 2; ++b) {
+    if (s.f[b]) cudaFree(s.f[b]);
+    if (s.db[b]) cudaFree(s.db[b]);
+    s.f[b] = s.db[b] = nullptr;
+  }
+  if (s.d_lat) cudaFree(s.d_lat);
+  if (s.d_tiles) cudaFree(s.d_tiles);
+  s.d_lat = nullptr;
+  s.d_tiles = nullptr;
+}
+
+int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const double *n,
+                const double *db, const uint8_t *rockp, cudaStream_t st) {
+  const long long N = P.nsites;
+  const double rho0 = s.lat.rho0;
+  std::vector<float> h((size_t)P.nc * 19 * N);
+  for (int c = 0; c < P.nc; ++c)
+    for (int q = 0; q < 19; ++q) {
+      const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * (double)rho0;
+      for (long long i = 0; i < N; ++i)
+        h[((size_t)c * 19 + q) * N + i] = (float)(n[((size_t)c * 19 + q) * N + i] - w);
+    }
+  // rock flag: any rock site present?
+  std::vector<uint8_t> rk(N);
+  if (cudaMemcpyAsync(rk.data(), rockp, N, cudaMemcpyDeviceToHost, st) != cudaSuccess) return LB3DC_ECUDA;
+  cudaStreamSynchronize(st);
+  bool any = false;
+  for (long long i = 0; i < N; ++i) any |= rk[i] != 0;
+  if (any && P.nc == 3) return LB3DC_EINVAL;
+  int parity = 0;
+  s.lat = fp32_make_desc(P, rho0, 0, any);
+  s.lat.parity = parity;
+  for (int b = 0; b < 2; ++b) {
+    if (cudaMemcpyAsync(s.f[b], h.data(), h.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return LB3DC_ECUDA;
+    if (P.nc == 3) {
+      std::vector<float> d(3 * N);
+      for (long long i = 0; i < 3 * N; ++i) d[i] = (float)db[i];
+      if (cudaMemcpyAsync(s.db[b], d.data(), d.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return LB3DC_ECUDA;
+      cudaStreamSynchronize(st);
+    }
+  }
+  if (cudaMemcpyAsync(s.d_lat, &s.lat, sizeof(LatDesc), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return LB3DC_ECUDA;
+  int rc = rebuild_tiles(P, s, default_shape(P), st);
+  if (rc) return rc;
+  return cudaStreamSynchronize(st) == cudaSuccess ? LB3DC_OK : LB3DC_ECUDA;
+}
+
+int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, double *n, double *db,
+                  double *rho, double *mom, double *da, const uint8_t *rockp, cudaStream_t st) {
+  const long long N = P.nsites;
+  const int nc = P.nc;
+  const int cur = s.lat.parity;
+  std::vector<float> h((size_t)nc * 19 * N);
+  if (cudaMemcpyAsync(h.data(), s.f[cur], h.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return LB3DC_ECUDA;
+  std::vector<float> d(nc == 3 ? 3 * N : 0);
+  if (nc == 3 && cudaMemcpyAsync(d.data(), s.db[cur], d.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return LB3DC_ECUDA;
+  std::vector<uint8_t> rk(N, 0);
+  if (rockp && cudaMemcpyAsync(rk.data(), rockp, N, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return LB3DC_ECUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return LB3DC_ECUDA;
+  const double rho0 = s.lat.rho0;
+  for (long long i = 0; i < N; ++i) {
+    for (int c = 0; c < nc; ++c) {
+      double r = 0, m0 = 0, m1 = 0, m2 = 0;
+      for (int q = 0; q < 19; ++q) {
+        const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+        // rock sites hold no populations (code/lb3d_ic_rock.F90:163-170)
+        const double v = rk[i] ? 0.0 : (double)h[((size_t)c * 19 + q) * N + i] + w;
+        if (n) n[((size_t)c * 19 + q) * N + i] = v;
+        const double ng = v * gw(q);
+        r += ng;
+        m0 += ng * cx(q);
+        m1 += ng * cy(q);
+        m2 += ng * cz(q);
+      }
+      if (rho) rho[(size_t)c * N + i] = r;
+      if (mom) {
+        mom[((size_t)c * 3 + 0) * N + i] = m0;
+        mom[((size_t)c * 3 + 1) * N + i] = m1;
+        mom[((size_t)c * 3 + 2) * N + i] = m2;
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      if (db) db[(size_t)k * N + i] = nc == 3 ? (double)d[(size_t)k * N + i] : 0.0;
+      if (da) da[(size_t)k * N + i] = 0.0;
+    }
+  }
+  (void)p;
+  return LB3DC_OK;
+}
+
+int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_t st) {
+  return fp32_run(P, s, rock, 1, st);
+}
+
+int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st) {
+  FusedShape sh{s.tx, s.ty, s.zc};
+  const bool rk = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
+  for (int i = 0; i < nsteps; ++i) {
+    if (s.timer) s.timer->start(st);
+    cudaError_t e = fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, s.grid,
+                                      s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st);
+    if (s.timer) {
+      s.timer->stop(st);
+      s.timer->launches += 2;
+    }
+    if (e != cudaSuccess) return LB3DC_ECUDA;
+    e = fp32_flip_parity(s.d_lat, 1, st);
+    if (e != cudaSuccess) return LB3DC_ECUDA;
+    s.lat.parity ^= 1;
+  }
+  return LB3DC_OK;
+}
+
+// Dumps of the FP32 state: the deviations are converted to FP64
+// populations on the device and the FP64 dump kernels are applied, with the
+// densities recomputed from the current populations (the FP32 path does not
+// keep the post-stream moments between steps).
+int fp32_dump(const DevParams &P, Fp32State &s, int field, const uint8_t *rock, double *out,
+              cudaStream_t st) {
+  const long long N = P.nsites;
+  const int nc = P.nc;
+  double *n = nullptr, *rho = nullptr, *psi = nullptr, *mom = nullptr, *db = nullptr;
+  size_t bytes = ((size_t)nc * 19 * N + 2 * (size_t)nc * N + 3 * (size_t)nc * N + 3 * (size_t)N) * 8;
+  if (cudaMalloc(&n, bytes) != cudaSuccess) return LB3DC_ENOMEM;
+  rho = n + (size_t)nc * 19 * N;
+  psi = rho + (size_t)nc * N;
+  mom = psi + (size_t)nc * N;
+  db = mom + 3 * (size_t)nc * N;
+  const int cur = s.lat.parity;
+  k_to_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.f[cur], n, s.S, 0, N, nc, s.lat.rho0);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = fp64_moments(P, n, rho, psi, mom, st);
+  if (e == cudaSuccess && nc == 3) {
+    std::vector<float> h(3 * N);
+    std::vector<double> hd(3 * N);
+    e = cudaMemcpyAsync(h.data(), s.db[cur], 3 * N * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    for (long long i = 0; i < 3 * N; ++i) hd[i] = h[i];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, hd.data(), 3 * N * 8, cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess) e = fp64_dump(P, field, n, rho, psi, db, rock, out, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(n);
+  return e == cudaSuccess ? LB3DC_OK : LB3DC_ECUDA;
+}
+
+cudaError_t fp32_reduce_conservation(const DevParams &P, Fp32State &s, const uint8_t *rock,
+                                     double *scratch, double mass[3], double mom[3],
+                                     cudaStream_t st) {
+  // Download-based FP64 sums (reduction over the host copy in FP64).
+  const long long N = P.nsites;
+  std::vector<double> n((size_t)P.nc * 19 * N);
+  lb3dc_params dummy{};
+  int rc = fp32_download(P, dummy, s, n.data(), nullptr, nullptr, nullptr, nullptr, rock, st);
+  (void)scratch;
+  if (rc) return cudaErrorUnknown;
+  std::vector<uint8_t> rk(N);
+  cudaMemcpyAsync(rk.data(), rock, N, cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  for (int k = 0; k < 3; ++k) mass[k] = mom[k] = 0.0;
+  for (long long i = 0; i < N; ++i) {
+    if (rk[i]) continue;
+    for (int c = 0; c < P.nc; ++c)
+      for (int q = 0; q < 19; ++q) {
+        double ng = n[((size_t)c * 19 + q) * N + i] * gw(q);
+        mass[c] += ng;
+        mom[0] += ng * cx(q);
+        mom[1] += ng * cy(q);
+        mom[2] += ng * cz(q);
+      }
+  }
+  return cudaSuccess;
+}
+
+cudaError_t fp32_sanity_counts(const DevParams &P, Fp32State &s, unsigned long long *scratch,
+                               unsigned long long cnt[2], cudaStream_t st) {
+  (void)scratch;
+  const long long N = P.nsites;
+  std::vector<double> n((size_t)P.nc * 19 * N);
+  lb3dc_params dummy{};
+  if (fp32_download(P, dummy, s, n.data(), nullptr, nullptr, nullptr, nullptr, nullptr, st))
+    return cudaErrorUnknown;
+  cnt[0] = cnt[1] = 0;
+  for (double v : n) {
+    if (!std::isfinite(v)) ++cnt[0];
+    else if (v < 0) ++cnt[1];
+  }
+  return cudaSuccess;
 }
 
 }  // namespace lb3d

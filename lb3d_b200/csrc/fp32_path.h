@@ -1,27 +1,67 @@
-// fp32_path.h -- the FP32 deviation-storage path (LB3DC_FP32_DEV).
+// fp32_path.h -- the FP32 deviation-storage path (LB3DC_FP32_DEV) and the
+// packed multi-lattice layout it shares with the ensemble runtime.
 #ifndef LB3D_FP32_PATH_H
 #define LB3D_FP32_PATH_H
+
+#include <vector>
 
 #include "common.cuh"
 
 namespace lb3d {
 
+// One lattice inside the packed arrays.  Populations are stored as FP32
+// deviations delta = n - w_i rho0 in f[c][q][S] with a global stride S
+// (the capacity in sites); lattice sites start at `base`.
+struct LatDesc {
+  int nx, ny, nz, nc;
+  long long base;
+  int parity;     // buffer holding the current state (0/1)
+  int flags;      // LAT_ROCK | LAT_BODY | LAT_ACTIVE
+  float omega[3], tau[3], amass[3];
+  float g_br, g_bs, g_ss;
+  float wall_r, wall_b;  // -g_wr tau_wr / tau_r and -g_wb tau_wb / tau_b
+  float psiw_r, psiw_b;  // psi(rock colour) seen from a fluid site
+  float beta, d0, omega_d;
+  float g_accn, g_accn_x, g_accn_y;
+  int amin_x, amax_x, amin_y, amax_y, amin_z, amax_z, inv_fluid;
+  float rho0, psi0, em0;  // psi(rho0) = 1 - exp(-rho0), em0 = exp(-rho0)
+};
+constexpr int LAT_ROCK = 1, LAT_BODY = 2, LAT_ACTIVE = 4;
+
+// Tile: lattice id, xy origin and z range of one CTA work item.
+struct Tile {
+  int lat;
+  short x0, y0;
+  short z0, zc;
+};
+
 struct Fp32State {
-  float *fa = nullptr, *fb = nullptr;  // deviation populations, ping-pong [nc][19][N]
-  float *da_ = nullptr, *db_a = nullptr, *db_b = nullptr;
-  double rho0 = 0.7;
-  int cur = 0;
+  float *f[2] = {nullptr, nullptr};   // [nc][19][S]
+  float *db[2] = {nullptr, nullptr};  // [3][S] (ternary)
+  LatDesc *d_lat = nullptr;
+  Tile *d_tiles = nullptr;
+  int ntiles = 0;
+  LatDesc lat{};        // host copy (single-lattice handle)
+  long long S = 0;      // stride (sites)
+  int tx = 32, ty = 8, zc = 16;  // launch shape (autotuned)
+  int grid = 0;
   long long bytes = 0;
-  void *aux = nullptr;
+  KernelTimer *timer = nullptr;  // optional, owned by the handle
+};
+
+// Launch configuration of the fused kernel.
+struct FusedShape {
+  int tx, ty, zc;
 };
 
 long long fp32_footprint(const lb3dc_params &p);
+LatDesc fp32_make_desc(const DevParams &P, double rho0, long long base, bool rock);
 int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStream_t st);
 void fp32_free(Fp32State &s);
 int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const double *n,
                 const double *db, const uint8_t *rock, cudaStream_t st);
 int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, double *n,
-                  double *db, double *rho, double *mom, double *da, double *scratch,
+                  double *db, double *rho, double *mom, double *da, const uint8_t *rock,
                   cudaStream_t st);
 int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_t st);
 int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st);
@@ -32,6 +72,23 @@ cudaError_t fp32_reduce_conservation(const DevParams &P, Fp32State &s, const uin
                                      cudaStream_t st);
 cudaError_t fp32_sanity_counts(const DevParams &P, Fp32State &s, unsigned long long *scratch,
                                unsigned long long cnt[2], cudaStream_t st);
+
+// Shared with the ensemble runtime: tile list for a lattice, fused launch.
+void fp32_tiles_for(const LatDesc &L, int lat_id, const FusedShape &sh, std::vector<Tile> &out);
+// fin/fout select by parity inside the kernel; `flip` is applied by caller.
+cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
+                              const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
+                              float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
+                              long long S, cudaStream_t st);
+// Flips the parity of every active lattice (one tiny kernel).
+cudaError_t fp32_flip_parity(LatDesc *d_lat, int nlat, cudaStream_t st);
+size_t fp32_fused_smem(int nc, const FusedShape &sh);
+int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st);
+// Candidate shapes of the autotuner.
+std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P);
+int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double *ms_out,
+                  int *ntried, cudaStream_t st);
+int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh);
 
 }  // namespace lb3d
 #endif

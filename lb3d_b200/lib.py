@@ -70,6 +70,12 @@ def lib():
         "lb3dc_collision": (I, [H]),
         "lb3dc_time_loop": (I, [H, I]),
         "lb3dc_sync": (I, [H]),
+        "lb3dc_set_launch_shape": (I, [H, I, I, I]),
+        "lb3dc_get_launch_shape": (I, [H, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "lb3dc_autotune": (I, [H, _D, ctypes.POINTER(I)]),
+        "lb3dc_stream": (ctypes.c_void_p, [H]),
+        "lb3dc_set_profiling": (I, [H, I]),
+        "lb3dc_kernel_stats": (I, [H, _D, ctypes.POINTER(LL), ctypes.POINTER(LL)]),
         "lb3dc_set_lees_edwards": (I, [H, Dd, Dd]),
         "lb3dc_get_lees_edwards": (I, [H, _D, _D]),
         "lb3dc_get_timestep": (I, [H, ctypes.POINTER(I)]),
@@ -210,6 +216,38 @@ class Lattice:
 
     def sync(self):
         self._ck(lib().lb3dc_sync(self.h))
+
+    # -- FP32 launch shape ------------------------------------------------
+    def set_launch_shape(self, tx, ty, zc):
+        self._ck(lib().lb3dc_set_launch_shape(self.h, int(tx), int(ty), int(zc)))
+
+    @property
+    def launch_shape(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().lb3dc_get_launch_shape(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def autotune(self):
+        ms = np.zeros(32)
+        n = ctypes.c_int()
+        self._ck(lib().lb3dc_autotune(self.h, ptr(ms), ctypes.byref(n)))
+        return self.launch_shape, ms[: n.value].tolist()
+
+    # -- measurement ------------------------------------------------------
+    @property
+    def stream(self):
+        return lib().lb3dc_stream(self.h)
+
+    def set_profiling(self, on=True):
+        self._ck(lib().lb3dc_set_profiling(self.h, int(bool(on))))
+
+    def kernel_stats(self):
+        """(device ms of the bracketed dominant kernels, their launch count,
+        all kernel launches issued) since set_profiling."""
+        ms = ctypes.c_double()
+        n, alln = ctypes.c_longlong(), ctypes.c_longlong()
+        self._ck(lib().lb3dc_kernel_stats(self.h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(alln)))
+        return ms.value, n.value, alln.value
 
     @property
     def timestep(self):
