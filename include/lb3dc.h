@@ -197,6 +197,37 @@ int lb3dc_xdr_write_rock(const char *path, int nx, int ny, int nz, const double 
 int lb3dc_xdr_write_field(const char *path, const double *v, long long nsites,
                           int values_per_site, int dump_double);
 
+/* ---- FP64 step without device allocation ------------------------------ */
+/* No counterpart in the reference.  For callers that may not call
+ * cudaMalloc -- code running while a stream is captured into a CUDA graph,
+ * hosts that own all device memory through their own pool or arrays (for
+ * instance a Fortran code keeping its lattice in its own device arrays), or
+ * loops that cannot take the synchronisation an allocation can imply.
+ * Runs nsteps periodic FP64 steps (the same kernels and results as
+ * lb3dc_time_loop with precision LB3DC_FP64) on device buffers the caller
+ * owns:
+ *   f    : [ncomp][19][nz][ny][nx] populations, in/out (rock sites must hold
+ *          zeros, as after lbe_init_rock_colour)
+ *   db   : [3][nz][ny][nx] dipoles, in/out (ternary; NULL for binary)
+ *   rock : [nz][ny][nx] uint8 rock mask, or NULL for none
+ *   stream : a cudaStream_t, or NULL for the default stream.
+ * It allocates nothing: the step's intermediate fields live in one
+ * file-scope device array of LB3DC_NOALLOC_SCRATCH_BYTES (32 MiB), which
+ * every GPU that loads the library holds until the process exits.  That
+ * bounds the lattice to 87380 binary or 55923 ternary sites (384 or 600
+ * scratch bytes per site; 87152 / 55829 without a caller rock mask); larger
+ * lattices are rejected with LB3DC_EINVAL and a message for
+ * lb3dc_last_error(NULL, ...).  Lees-Edwards and FP32 are not offered here.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the one array and it keeps the last call's
+ * contents: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Asynchronous on
+ * `stream`; returns after enqueueing. */
+#define LB3DC_NOALLOC_SCRATCH_BYTES (32ull * 1024ull * 1024ull)
+int lb3dc_time_loop_fp64_noalloc(const lb3dc_params *p, double *f, double *db,
+                                 const unsigned char *rock, int nsteps, void *stream);
+
 /* ---- self-test helpers ------------------------------------------------- */
 /* Evaluates the deterministic FP64 exp (fn 0), expm1 (1) or tanh (2) of
  * the FP64 path on the host (device = 0) or on the current CUDA device

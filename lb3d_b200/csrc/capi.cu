@@ -13,6 +13,7 @@
 #include "detmath.h"
 #include "fp32_path.h"
 #include "fp64_path.h"
+#include "params.h"
 #include "reduce.h"
 
 using namespace lb3d;
@@ -218,6 +219,12 @@ int ensure_scratch(lb3dc_handle *h, long long bytes) {
 }
 
 }  // namespace
+
+namespace lb3d {
+int validate_params(const lb3dc_params *p, std::string &why) { return validate(p, why); }
+DevParams dev_params_from(const lb3dc_params &p) { return make_dev_params(p); }
+int set_global_error(int code, const char *msg) { return fail(nullptr, code, "%s", msg); }
+}  // namespace lb3d
 
 extern "C" {
 
