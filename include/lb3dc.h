@@ -197,6 +197,50 @@ int lb3dc_xdr_write_rock(const char *path, int nx, int ny, int nz, const double 
 int lb3dc_xdr_write_field(const char *path, const double *v, long long nsites,
                           int values_per_site, int dump_double);
 
+/* ---- ensembles: many lattices, one persistent kernel ------------------- */
+/*
+ * Parameter sweeps (many independent small lattices of uneven size) run as
+ * one ensemble: every member occupies a contiguous range of one packed,
+ * device-resident site space and all active members advance together in
+ * the FP32 deviation path's fused kernel over one tile list, replayed from a
+ * CUDA graph while the active set is unchanged.  A member's results are the
+ * same alone and in any mix.  No counterpart in the reference (which runs
+ * one lattice per MPI job); the per-lattice arithmetic is that of the
+ * single-lattice FP32 path.
+ */
+typedef struct lb3dc_ensemble lb3dc_ensemble;
+/* capacity_sites bounds the sum of member sizes (19*ncomp*capacity < 2^31);
+ * device bytes: 2*19*ncomp*4 (+24 ternary) per site of capacity. */
+int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
+                          lb3dc_ensemble **out);
+int lb3dc_ensemble_destroy(lb3dc_ensemble *e);
+int lb3dc_ensemble_last_error(const lb3dc_ensemble *e, char *buf, int len);
+int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc);
+/* Admits one periodic lattice (p->precision is ignored: members are FP32
+ * deviation) that will run nsteps steps; n, db as in lb3dc_upload_state.
+ * Returns LB3DC_ENOMEM when no slot or no contiguous site range is free:
+ * the caller keeps the request queued (admission by HBM footprint). */
+int lb3dc_ensemble_admit(lb3dc_ensemble *e, const lb3dc_params *p, const double *n,
+                         const double *db, int nsteps, int *slot_out);
+/* As lb3dc_ensemble_admit, with the seeded initial state generated on the
+ * device: rho_c = rho[c] + U(-amp, amp) per site from the SplitMix64
+ * counter generator of lb3d_b200/ic.py, zero velocity, unit dipoles. */
+int lb3dc_ensemble_admit_seeded(lb3dc_ensemble *e, const lb3dc_params *p, unsigned long long seed,
+                                const double rho[3], double amp, int nsteps, int *slot_out);
+/* Advances every active member by up to max_steps steps, stopping early when
+ * the first member completes its steps; *steps_done receives the count.
+ * Asynchronous. */
+int lb3dc_ensemble_step(lb3dc_ensemble *e, int max_steps, int *steps_done);
+int lb3dc_ensemble_sync(lb3dc_ensemble *e);
+/* Members that completed their steps (still resident until retired). */
+int lb3dc_ensemble_finished(lb3dc_ensemble *e, int *slots, int max, int *count);
+/* Downloads a member's populations/dipoles (either may be NULL) and frees
+ * its slot and site range (synchronising). */
+int lb3dc_ensemble_retire(lb3dc_ensemble *e, int slot, double *n, double *db);
+int lb3dc_ensemble_stats(const lb3dc_ensemble *e, long long *free_sites, int *active,
+                         int *resident, long long *site_updates);
+long long lb3dc_ensemble_bytes(const lb3dc_ensemble *e);
+
 /* ---- FP64 step without device allocation ------------------------------ */
 /* No counterpart in the reference.  For callers that may not call
  * cudaMalloc -- code running while a stream is captured into a CUDA graph,

@@ -118,17 +118,20 @@ __device__ __forceinline__ int noff(const Nbr &n) {
 // delta*(x, bounce(q)) when x - c_q is rock (code/lb3d_bc_bounce.F90:53-90
 // with code/lb3d_advection.F90:109-151).  F points at component 0 of the
 // lattice; the component stride is 19*S.
-template <bool ROCK>
+// LAST selects the last-use load hint (the final read of these values by
+// this CTA), which lets L2 drop the lines early.
+template <bool ROCK, bool LAST = false>
 __device__ __forceinline__ void pull_comp(const float *__restrict__ F, int S, int c, const Nbr &n,
                                           int self, const uint8_t *__restrict__ rk, float d[19]) {
   const float *fc = F + c * 19 * S;
-  d[18] = __ldg(fc + 18 * S + self);
+  d[18] = LAST ? __ldlu(fc + 18 * S + self) : __ldg(fc + 18 * S + self);
 #define LB3D_PULL(Q)                                                     \
   {                                                                      \
     const int up = noff<Q, -1>(n);                                       \
     bool uf = true;                                                      \
     if (ROCK) uf = __ldg(rk + up) == 0;                                  \
-    d[Q] = __ldg(fc + (uf ? Q * S + up : bounce(Q) * S + self));         \
+    const float *a_ = fc + (uf ? Q * S + up : bounce(Q) * S + self);     \
+    d[Q] = LAST ? __ldlu(a_) : __ldg(a_);                                \
   }
   LB3D_PULL(0) LB3D_PULL(1) LB3D_PULL(2) LB3D_PULL(3) LB3D_PULL(4) LB3D_PULL(5)
   LB3D_PULL(6) LB3D_PULL(7) LB3D_PULL(8) LB3D_PULL(9) LB3D_PULL(10) LB3D_PULL(11)
@@ -140,24 +143,45 @@ __device__ __forceinline__ void pull_comp(const float *__restrict__ F, int S, in
 // The fused kernel.  Grid: persistent CTAs over a tile list.  Populations
 // of lattice L live at f[(c*19+q)*S + L.base + site]; offsets are 32-bit,
 // which bounds the packed capacity at 19*nc*S < 2^31.
+//
+// On-chip rings (float4 entries, one per site):
+//   A  ternary: {rho_b - rho_r, drho_s, da_x, da_y}, {da_z, dpsi_r, dpsi_b,
+//      dpsi_s} on the tile + 2 halo, 4 planes;  binary: {dpsi_r, dpsi_b, -, -}
+//      on the tile + 1 halo, 3 planes
+//   B  ternary: new dipoles {d_x, d_y, d_z, -} on the tile + 1 halo, 3 planes
+//   D  ternary: previous dipoles on the tile + 3 halo, 3 planes
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int wrap_small(int v, int n) {
+  // valid for -n <= v < 2n
+  return v < 0 ? v + n : (v >= n ? v - n : v);
+}
+
+template <int NC, int TX, int TY>
+struct FusedGeom {
+  static constexpr int NT = TX * TY;
+  static constexpr int H = (NC == 3) ? 2 : 1;
+  static constexpr int AW = TX + 2 * H, AH = TY + 2 * H, AN = AW * AH;
+  static constexpr int AV = (NC == 3) ? 2 : 1;  // float4 per A entry
+  static constexpr int AR = (NC == 3) ? 4 : 3;  // A ring depth
+  static constexpr int BW = TX + 2, BH = TY + 2, BN = BW * BH;
+  static constexpr int DW = TX + 6, DH = TY + 6, DN = DW * DH;
+  static constexpr int A_F4 = AR * AV * AN;
+  static constexpr int B_F4 = (NC == 3) ? 3 * BN : 0;
+  static constexpr int D_F4 = (NC == 3) ? 3 * DN : 0;
+  static constexpr int SMEM = 16 * (A_F4 + B_F4 + D_F4);
+};
+
 template <int NC, int TX, int TY, bool ROCK, bool BODY>
-__global__ void __launch_bounds__(TX *TY, 1)
+__global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 ? 2 : 3)))
     k_fused(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
             float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, int S) {
-  constexpr int NT = TX * TY;
-  constexpr int H = (NC == 3) ? 2 : 1;  // halo of the moment stage
-  constexpr int AW = TX + 2 * H, AH = TY + 2 * H, AN = AW * AH;
-  constexpr int AF = (NC == 3) ? 8 : 2;  // fields per A entry
-  constexpr int AR = (NC == 3) ? 4 : 3;  // A ring depth
-  constexpr int BW = TX + 2, BH = TY + 2, BN = BW * BH;
-  constexpr int DW = TX + 6, DH = TY + 6, DN = DW * DH;
-  // A fields (ternary): 0 rho_b - rho_r, 1 drho_s, 2..4 da, 5 dpsi_r,
-  // 6 dpsi_b, 7 dpsi_s.   Binary: 0 dpsi_r, 1 dpsi_b.
-  extern __shared__ float smem[];
-  float *ringA = smem;                                  // [AR][AF][AN]
-  float *ringB = ringA + AR * AF * AN;                  // [3][3][BN]   (ternary)
-  float *ringD = ringB + ((NC == 3) ? 3 * 3 * BN : 0);  // [3][3][DN]   (ternary)
+  using G = FusedGeom<NC, TX, TY>;
+  constexpr int NT = G::NT, H = G::H, AW = G::AW, AN = G::AN, AV = G::AV, AR = G::AR;
+  constexpr int BW = G::BW, BN = G::BN, DW = G::DW, DN = G::DN;
+  extern __shared__ float4 smem4[];
+  float4 *ringA = smem4;              // [AR][AV][AN]
+  float4 *ringB = ringA + G::A_F4;    // [3][BN]
+  float4 *ringD = ringB + G::B_F4;    // [3][DN]
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
 
@@ -176,18 +200,19 @@ __global__ void __launch_bounds__(TX *TY, 1)
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
     const int zfirst = z0 - H;
     const int niter = zc + 2 * H;
+    // halo coordinates stay within one period of the lattice when the
+    // lattice is at least a tile plus halo wide; otherwise use modulo
+    const bool small = (nx < TX + 3) || (ny < TY + 3);
+    auto wx = [&](int v) { return small ? pmod(v, nx) : wrap_small(v, nx); };
+    auto wy = [&](int v) { return small ? pmod(v, ny) : wrap_small(v, ny); };
 
-    // ternary: previous dipoles of one plane (with a 3-site xy halo) into
-    // the D ring; plane zfirst - 1 + j goes to slot j % 3.
     auto load_db_plane = [&](int j) {
       const int gz = pmod(zfirst - 1 + j, nz);
-      float *dst = ringD + (j % 3) * 3 * DN;
+      float4 *dst = ringD + (j % 3) * DN;
       for (int s = tid; s < DN; s += NT) {
-        const int gx = pmod(x0 - 3 + s % DW, nx), gy = pmod(y0 - 3 + s / DW, ny);
+        const int gx = wx(x0 - 3 + s % DW), gy = wy(y0 - 3 + s / DW);
         const int i = gx + nx * (gy + ny * gz);
-        dst[s] = __ldg(DBi + i);
-        dst[DN + s] = __ldg(DBi + S + i);
-        dst[2 * DN + s] = __ldg(DBi + 2 * S + i);
+        dst[s] = make_float4(__ldg(DBi + i), __ldg(DBi + S + i), __ldg(DBi + 2 * S + i), 0.0f);
       }
     };
     if (NC == 3) {
@@ -201,11 +226,15 @@ __global__ void __launch_bounds__(TX *TY, 1)
       __syncthreads();
       // ---------------- stage A: post-stream moments on the haloed tile ----
       {
-        float *slot = ringA + (it % AR) * AF * AN;
+        float4 *slot = ringA + (it % AR) * AV * AN;
         const int gz = pmod(zA, nz);
+        // D ring: plane zfirst - 1 + j sits in slot j % 3
+        const float4 *Dm = ringD + (it % 3) * DN;        // plane zA - 1
+        const float4 *D0 = ringD + ((it + 1) % 3) * DN;  // plane zA
+        const float4 *Dp = ringD + ((it + 2) % 3) * DN;  // plane zA + 1
         for (int s = tid; s < AN; s += NT) {
           const int ax = s % AW, ay = s / AW;
-          const int gx = pmod(x0 - H + ax, nx), gy = pmod(y0 - H + ay, ny);
+          const int gx = wx(x0 - H + ax), gy = wy(y0 - H + ay);
           Nbr nb;
           make_nbr(nb, gx, gy, gz, nx, ny, nz);
           const int self = noff<18, 1>(nb);
@@ -217,66 +246,64 @@ __global__ void __launch_bounds__(TX *TY, 1)
             pull_comp<ROCK>(F, S, c, nb, self, RK, d);
             float acc = 0.0f;
 #pragma unroll
-            for (int q = 0; q < 19; ++q) acc += (float)gw(q) * d[q];
+            for (int q = 0; q < 19; ++q) acc = fmaf((float)gw(q), d[q], acc);
             dr[c] = acc;
             if (NC == 3 && c == 2) {
               // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
               // (code/lb3d_advection.F90:137-148)
-              const int dx = ax + 1, dy = ay + 1;  // A-local -> D-local
+              const int ds0 = (ax + 1) + DW * (ay + 1);  // A-local -> D-local
 #pragma unroll
               for (int q = 0; q < 19; ++q) {
-                const float *Dp = ringD + ((it + 1 - cz(q)) % 3) * 3 * DN;
-                const int ds = (dx - cx(q)) + DW * (dy - cy(q));
+                const float4 *Dq = cz(q) == 1 ? Dm : (cz(q) == -1 ? Dp : D0);
+                const float4 b = Dq[ds0 - cx(q) - DW * cy(q)];
                 const float ng = (float)gw(q) * (d[q] + wq(q) * rho0);
-                a0 = fmaf(ng, Dp[ds], a0);
-                a1 = fmaf(ng, Dp[DN + ds], a1);
-                a2 = fmaf(ng, Dp[2 * DN + ds], a2);
+                a0 = fmaf(ng, b.x, a0);
+                a1 = fmaf(ng, b.y, a1);
+                a2 = fmaf(ng, b.z, a2);
               }
             }
           }
           if (NC == 3) {
-            slot[0 * AN + s] = dr[1] - dr[0];
-            slot[1 * AN + s] = dr[NC - 1];
-            slot[2 * AN + s] = a0;
-            slot[3 * AN + s] = a1;
-            slot[4 * AN + s] = a2;
-            slot[5 * AN + s] = -em0 * expm1f(-dr[0]);
-            slot[6 * AN + s] = -em0 * expm1f(-dr[1]);
-            slot[7 * AN + s] = -em0 * expm1f(-dr[NC - 1]);
+            slot[s] = make_float4(dr[1] - dr[0], dr[NC - 1], a0, a1);
+            slot[AN + s] = make_float4(a2, -em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]),
+                                       -em0 * expm1f(-dr[NC - 1]));
           } else {
-            slot[0 * AN + s] = -em0 * expm1f(-dr[0]);
-            slot[1 * AN + s] = -em0 * expm1f(-dr[1]);
+            slot[s] = make_float4(-em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]), 0.f, 0.f);
           }
         }
       }
       __syncthreads();
       // ---------------- stage B (ternary): dipole relaxation ----------------
       if (NC == 3 && it >= 2) {
-        float *slotB = ringB + (it % 3) * 3 * BN;
+        float4 *slotB = ringB + (it % 3) * BN;
         const int zB = zA - 1;
         const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
-        const float *Ac = ringA + ((it - 1) % AR) * AF * AN;
+        const float4 *Am = ringA + ((it - 2) % AR) * AV * AN;  // plane zB - 1
+        const float4 *A0 = ringA + ((it - 1) % AR) * AV * AN;  // plane zB
+        const float4 *Ap = ringA + ((it) % AR) * AV * AN;      // plane zB + 1
         for (int s = tid; s < BN; s += NT) {
           const int bx = s % BW, by = s / BW;
           const int as = (bx + 1) + AW * (by + 1);
+          const float4 own0 = A0[as];
+          const float own_daz = A0[AN + as].x;
           float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
-          float hs0 = Ac[2 * AN + as], hs1 = Ac[3 * AN + as], hs2 = Ac[4 * AN + as];
-          const float isN = 1.0f / fmaxf(rho0 + Ac[1 * AN + as], 1.0e-4f);
-          const float st0 = hs0 * isN, st1 = hs1 * isN, st2 = hs2 * isN;
+          float hs0 = own0.z, hs1 = own0.w, hs2 = own_daz;
+          const float isN = 1.0f / fmaxf(rho0 + own0.y, 1.0e-4f);
 #pragma unroll
           for (int q = 0; q < 18; ++q) {
-            const float *Ap = ringA + ((it - 1 + cz(q)) % AR) * AF * AN;
+            const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
             const int an = as + cx(q) + AW * cy(q);
+            const float4 e0 = Aq[an];
+            const float pz = Aq[AN + an].x;
             const float g = (float)gw(q);
-            const float hcm = -sgn * Ap[an] * g;  // field 0 = rho_b - rho_r
-            const float p0 = Ap[2 * AN + an], p1 = Ap[3 * AN + an], p2 = Ap[4 * AN + an];
-            const float dot2 = 2.0f * (cx(q) * p0 + cy(q) * p1 + cz(q) * p2);
-            hc0 += hcm * cx(q);
-            hc1 += hcm * cy(q);
-            hc2 += hcm * cz(q);
-            hs0 += (p0 - cx(q) * dot2) * g;
-            hs1 += (p1 - cy(q) * dot2) * g;
-            hs2 += (p2 - cz(q) * dot2) * g;
+            const float hcm = -sgn * e0.x * g;  // e0.x = rho_b - rho_r
+            const float dot2 = 2.0f * (cx(q) * e0.z + cy(q) * e0.w + cz(q) * pz);
+            if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
+            if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
+            if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
+            hs0 = fmaf(e0.z - cx(q) * dot2, g, hs0);
+            hs1 = fmaf(e0.w - cy(q) * dot2, g, hs1);
+            hs2 = fmaf(pz - cz(q) * dot2, g, hs2);
           }
           const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
           const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
@@ -284,21 +311,19 @@ __global__ void __launch_bounds__(TX *TY, 1)
           // d_eq = d0 L(beta|h|) h/|h| with the Langevin function L; the
           // reference's small-field branch beta h / 3 (h_m <= 0.01) is L's
           // first-order term.
-          float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
-          const float od = Lg.omega_d, om1 = 1.0f - od;
-          const float n0 = od * fac * h0 + om1 * st0;
-          const float n1 = od * fac * h1 + om1 * st1;
-          const float n2 = od * fac * h2 + om1 * st2;
-          slotB[s] = n0;
-          slotB[BN + s] = n1;
-          slotB[2 * BN + s] = n2;
+          const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
+          const float od = Lg.omega_d, om1 = (1.0f - od) * isN;
+          const float n0 = od * fac * h0 + om1 * own0.z;
+          const float n1 = od * fac * h1 + om1 * own0.w;
+          const float n2 = od * fac * h2 + om1 * own_daz;
+          slotB[s] = make_float4(n0, n1, n2, 0.0f);
           if (bx >= 1 && bx <= TX && by >= 1 && by <= TY && zB >= z0 && zB < z0 + zc) {
             const int gx = x0 + bx - 1, gy = y0 + by - 1;
             if (gx < nx && gy < ny) {
               const int i = gx + nx * (gy + ny * pmod(zB, nz));
-              DBo[i] = n0;
-              DBo[S + i] = n1;
-              DBo[2 * S + i] = n2;
+              __stcs(DBo + i, n0);
+              __stcs(DBo + S + i, n1);
+              __stcs(DBo + 2 * S + i, n2);
             }
           }
         }
@@ -318,91 +343,124 @@ __global__ void __launch_bounds__(TX *TY, 1)
           if (ROCK) own_rock = __ldg(RK + self) != 0;
           if (!own_rock) {
             const int as = (tx + H) + AW * (ty + H);
-            const float *A0 = ringA + (itC % AR) * AF * AN;
+            const float4 *Am = ringA + ((itC + AR - 1) % AR) * AV * AN;
+            const float4 *A0 = ringA + (itC % AR) * AV * AN;
+            const float4 *Ap = ringA + ((itC + 1) % AR) * AV * AN;
             float Fx[NC][3];
             float psi_own[NC];
             if (NC == 3) {
-              // ---- ternary Shan-Chen force, code/lb3d_force_shanchen.F90:215-330
+              // ---- ternary Shan-Chen force, code/lb3d_force_shanchen.F90:215-330,
+              // accumulated as moments of the neighbour terms so that the own
+              // dipole d enters once at the end:
+              //   f_cs = SA - 2 V,            SA = sum g a,  V = sum g (a.c) c
+              //   f_sc = SG d - 2 T d,        SG = sum G, T = sum G c c^T, G = g (psi_b - psi_r)
+              //   f_ss = M^T d + M d + tr(M) d - 2 Q d,
+              //                               M = sum 8g a c^T, Q = sum 8g (a.c) c c^T
+              // with a = d(y) psi_s(y) the neighbour's dipole times its psi.
               const int itB = itC + 1;  // B computed plane zC at iteration itC + 1
               const int bs = (tx + 1) + BW * (ty + 1);
-              const float *B0 = ringB + (itB % 3) * 3 * BN;
-              const float d0x = B0[bs], d1x = B0[BN + bs], d2x = B0[2 * BN + bs];
-              float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fcs[3] = {0, 0, 0}, fsc[3] = {0, 0, 0},
-                    fss[3] = {0, 0, 0};
+              const float4 *Bm = ringB + ((itB + 2) % 3) * BN;
+              const float4 *B0 = ringB + (itB % 3) * BN;
+              const float4 *Bp = ringB + ((itB + 1) % 3) * BN;
+              float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, SA[3] = {0, 0, 0}, V[3] = {0, 0, 0};
+              float SG = 0.f, T[6] = {0, 0, 0, 0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0};
+              float M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
               for (int q = 0; q < 18; ++q) {
-                const float *Ap = ringA + ((itC + cz(q)) % AR) * AF * AN;
-                const float *Bp = ringB + ((itB + cz(q)) % 3) * 3 * BN;
+                const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
+                const float4 *Bq = cz(q) == 1 ? Bp : (cz(q) == -1 ? Bm : B0);
                 const int an = as + cx(q) + AW * cy(q);
                 const int bn = bs + cx(q) + BW * cy(q);
                 const float g = (float)gw(q);
-                const float c[3] = {(float)cx(q), (float)cy(q), (float)cz(q)};
-                const float pr = Ap[5 * AN + an], pb = Ap[6 * AN + an];
-                const float ps = psi0 + Ap[7 * AN + an];
-                const float a[3] = {Bp[bn] * ps, Bp[BN + bn] * ps, Bp[2 * BN + bn] * ps};
-                const float ddc = a[0] * c[0] + a[1] * c[1] + a[2] * c[2];
-                const float dic = d0x * c[0] + d1x * c[1] + d2x * c[2];
-                const float did = a[0] * d0x + a[1] * d1x + a[2] * d2x;
-                const float gcs = (pb - pr) * g;
-                const float dx[3] = {d0x, d1x, d2x};
-                const float s8 = 8.0f * g;
-                const float coef = did - 2.0f * dic * ddc;
+                const int c[3] = {cx(q), cy(q), cz(q)};
+                const float4 e = Aq[AN + an];  // {da_z, dpsi_r, dpsi_b, dpsi_s}
+                const float4 b = Bq[bn];
+                const float ps = psi0 + e.w;
+                const float a[3] = {b.x * ps, b.y * ps, b.z * ps};
+                float ac = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                  if (c[k]) ac = fmaf((float)c[k], a[k], ac);
+                const float Gq = g * (e.z - e.y);
+                const float g8 = 8.0f * g;
+                SG += Gq;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                  if (c[k] != 0.0f) {
-                    frb[k] = fmaf(pb * g, c[k], frb[k]);
-                    fbr[k] = fmaf(pr * g, c[k], fbr[k]);
+                  SA[k] = fmaf(g, a[k], SA[k]);
+                  if (c[k]) {
+                    frb[k] = fmaf(g * (float)c[k], e.z, frb[k]);
+                    fbr[k] = fmaf(g * (float)c[k], e.y, fbr[k]);
+                    V[k] = fmaf(g * (float)c[k], ac, V[k]);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) M[i][k] = fmaf(g8 * (float)c[k], a[i], M[i][k]);
                   }
-                  fcs[k] += (a[k] - 2.0f * ddc * c[k]) * g;
-                  fsc[k] = fmaf(gcs, dx[k] - 2.0f * dic * c[k], fsc[k]);
-                  fss[k] = fmaf(s8, coef * c[k] + a[k] * dic + ddc * dx[k], fss[k]);
                 }
+                // symmetric c c^T: entries xx yy zz xy xz yz
+#define LB3D_SYM(I, J, K)                                      \
+  if (c[I] && c[J]) {                                          \
+    const float cc = (float)(c[I] * c[J]);                     \
+    T[K] = fmaf(Gq, cc, T[K]);                                 \
+    Q[K] = fmaf(g8 * ac, cc, Q[K]);                            \
+  }
+                LB3D_SYM(0, 0, 0) LB3D_SYM(1, 1, 1) LB3D_SYM(2, 2, 2)
+                LB3D_SYM(0, 1, 3) LB3D_SYM(0, 2, 4) LB3D_SYM(1, 2, 5)
+#undef LB3D_SYM
               }
-              psi_own[0] = psi0 + A0[5 * AN + as];
-              psi_own[1] = psi0 + A0[6 * AN + as];
-              psi_own[NC - 1] = psi0 + A0[7 * AN + as];
+              const float4 dd = B0[bs];
+              const float d[3] = {dd.x, dd.y, dd.z};
+              const float4 own = A0[AN + as];
+              psi_own[0] = psi0 + own.y;
+              psi_own[1] = psi0 + own.z;
+              psi_own[NC - 1] = psi0 + own.w;
+              const float Td[3] = {T[0] * d[0] + T[3] * d[1] + T[4] * d[2],
+                                   T[3] * d[0] + T[1] * d[1] + T[5] * d[2],
+                                   T[4] * d[0] + T[5] * d[1] + T[2] * d[2]};
+              const float Qd[3] = {Q[0] * d[0] + Q[3] * d[1] + Q[4] * d[2],
+                                   Q[3] * d[0] + Q[1] * d[1] + Q[5] * d[2],
+                                   Q[4] * d[0] + Q[5] * d[1] + Q[2] * d[2]};
+              const float trM = M[0][0] + M[1][1] + M[2][2];
 #pragma unroll
               for (int k = 0; k < 3; ++k) {
-                const float cs = -2.0f * Lg.g_bs * fcs[k];
+                const float MTd = M[0][k] * d[0] + M[1][k] * d[1] + M[2][k] * d[2];
+                const float Md = M[k][0] * d[0] + M[k][1] * d[1] + M[k][2] * d[2];
+                const float fcs = SA[k] - 2.0f * V[k];
+                const float fsc = SG * d[k] - 2.0f * Td[k];
+                const float fss = MTd + Md + trM * d[k] - 2.0f * Qd[k];
+                const float cs = -2.0f * Lg.g_bs * fcs;
                 Fx[1][k] = (-Lg.g_br * fbr[k] + cs) * psi_own[1];
                 Fx[0][k] = (-Lg.g_br * frb[k] - cs) * psi_own[0];
-                Fx[NC - 1][k] = (2.0f * Lg.g_bs * fsc[k] - Lg.g_ss * fss[k]) * psi_own[NC - 1];
+                Fx[NC - 1][k] = (2.0f * Lg.g_bs * fsc - Lg.g_ss * fss) * psi_own[NC - 1];
               }
             } else {
               // ---- binary Shan-Chen force with walls, :127-210
               float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
 #pragma unroll
               for (int q = 0; q < 18; ++q) {
-                const float *Ap = ringA + ((itC + cz(q)) % AR) * AF * AN;
+                const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
                 const int an = as + cx(q) + AW * cy(q);
                 const float g = (float)gw(q);
-                const float c[3] = {(float)cx(q), (float)cy(q), (float)cz(q)};
+                const int c[3] = {cx(q), cy(q), cz(q)};
                 bool nrock = false;
                 if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
-                if (nrock) {
-                  // a rock neighbour contributes psi(0 + rock colour) to the
-                  // wall sums; the fluid sums run over fluid neighbours only,
-                  // so their psi(rho0) share no longer cancels and is removed.
+                // a rock neighbour contributes psi(0 + rock colour) to the
+                // wall sums; the fluid sums run over fluid neighbours only,
+                // so their psi(rho0) share no longer cancels and is removed.
+                const float4 e = Aq[an];
+                const float pr = nrock ? -psi0 : e.x, pb = nrock ? -psi0 : e.y;
 #pragma unroll
-                  for (int k = 0; k < 3; ++k)
-                    if (c[k] != 0.0f) {
-                      fwb[k] = fmaf(Lg.psiw_b * g, c[k], fwb[k]);
-                      fwr[k] = fmaf(Lg.psiw_r * g, c[k], fwr[k]);
-                      frb[k] = fmaf(-psi0 * g, c[k], frb[k]);
-                      fbr[k] = fmaf(-psi0 * g, c[k], fbr[k]);
+                for (int k = 0; k < 3; ++k)
+                  if (c[k]) {
+                    frb[k] = fmaf(pb * g, (float)c[k], frb[k]);
+                    fbr[k] = fmaf(pr * g, (float)c[k], fbr[k]);
+                    if (ROCK && nrock) {
+                      fwb[k] = fmaf(Lg.psiw_b * g, (float)c[k], fwb[k]);
+                      fwr[k] = fmaf(Lg.psiw_r * g, (float)c[k], fwr[k]);
                     }
-                } else {
-                  const float pr = Ap[0 * AN + an], pb = Ap[1 * AN + an];
-#pragma unroll
-                  for (int k = 0; k < 3; ++k)
-                    if (c[k] != 0.0f) {
-                      frb[k] = fmaf(pb * g, c[k], frb[k]);
-                      fbr[k] = fmaf(pr * g, c[k], fbr[k]);
-                    }
-                }
+                  }
               }
-              psi_own[0] = psi0 + A0[0 * AN + as];
-              psi_own[1] = psi0 + A0[1 * AN + as];
+              const float4 own = A0[as];
+              psi_own[0] = psi0 + own.x;
+              psi_own[1] = psi0 + own.y;
 #pragma unroll
               for (int k = 0; k < 3; ++k) {
                 Fx[1][k] = (-Lg.g_br * fbr[k] + Lg.wall_b * fwb[k]) * psi_own[1];
@@ -465,18 +523,20 @@ __global__ void __launch_bounds__(TX *TY, 1)
             }
             const float irt = 1.0f / fmaxf(rt, 1.0e-8f);
             const float u0 = p0 * irt, u1 = p1 * irt, u2 = p2 * irt;
-            // ---- pass 2: reload (L1), relax, store
+            // ---- pass 2: reload, relax, store
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
               // du = tau F / (amass max(rho, 1e-8))  (:523-556)
               const float k = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
               float d[19];
-              pull_comp<ROCK>(F, S, c, nb, self, RK, d);
+              pull_comp<ROCK, true>(F, S, c, nb, self, RK, d);
               bgk_update(d, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
                          fmaf(k, Fx[c][2], u2), Lg.omega[c]);
               float *fo = Fo + c * 19 * S + self;
+              // streaming stores: the new populations are not read again in
+              // this launch, so they should not displace the inputs from L2
 #pragma unroll
-              for (int q = 0; q < 19; ++q) fo[q * S] = d[q];
+              for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
             }
           }
         }
@@ -514,8 +574,8 @@ size_t fp32_fused_smem(int nc, const FusedShape &sh) {
   const size_t AN = (size_t)(sh.tx + 2 * H) * (sh.ty + 2 * H);
   const size_t BN = (size_t)(sh.tx + 2) * (sh.ty + 2);
   const size_t DN = (size_t)(sh.tx + 6) * (sh.ty + 6);
-  if (nc == 3) return 4 * (4 * 8 * AN + 3 * 3 * BN + 3 * 3 * DN);
-  return 4 * (3 * 2 * AN);
+  if (nc == 3) return 16 * (4 * 2 * AN + 3 * BN + 3 * DN);
+  return 16 * (3 * AN);
 }
 
 template <int NC, int TX, int TY, bool ROCK, bool BODY>
