@@ -135,14 +135,18 @@ int lb3dc_time_loop(lb3dc_handle *h, int nsteps);
 int lb3dc_sync(lb3dc_handle *h);
 
 /* ---- launch shape of the FP32 fused kernel ------------------------------ */
-/* Tile of the fused stream-collide kernel: tx x ty sites per CTA, zc planes
- * per work item.  Supported (tx,ty): (32,8) (32,4) (16,16) (16,8) (64,4). */
-int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc);
-int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc);
-/* Times every supported shape on this lattice (on a saved copy of the
- * state, which is restored afterwards) and keeps the fastest.  ms_out
- * (optional, length >= 32) receives the measured ms per step of each tried
- * shape in the order tried; returns the number tried in *ntried. */
+/* Tile of the FP32 kernels: tx x ty sites per CTA, zc planes per work
+ * item; supported (tx,ty): (32,8) (32,4) (16,16) (16,8) (64,4).  split
+ * selects the strategy: 0 = one fused stream-collide pass per step (the
+ * moments of the halo are recomputed on chip), 1 = a moments pass writing a
+ * per-site moment field (32 B ternary, 8 B binary) and a collide pass that
+ * reads it with its halo. */
+int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc, int split);
+int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc, int *split);
+/* Times every supported shape and strategy on this lattice (on a saved copy
+ * of the state, which is restored afterwards) and keeps the fastest.  ms_out
+ * (optional, length >= 64) receives the measured ms per step of each tried
+ * candidate in the order tried; returns the number tried in *ntried. */
 int lb3dc_autotune(lb3dc_handle *h, double *ms_out, int *ntried);
 
 /* ---- measurement ------------------------------------------------------ */
@@ -215,7 +219,7 @@ int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
                           lb3dc_ensemble **out);
 int lb3dc_ensemble_destroy(lb3dc_ensemble *e);
 int lb3dc_ensemble_last_error(const lb3dc_ensemble *e, char *buf, int len);
-int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc);
+int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc, int split);
 /* Admits one periodic lattice (p->precision is ignored: members are FP32
  * deviation) that will run nsteps steps; n, db as in lb3dc_upload_state.
  * Returns LB3DC_ENOMEM when no slot or no contiguous site range is free:

@@ -575,16 +575,17 @@ int lb3dc_kernel_stats(lb3dc_handle *h, double *ms_total, long long *launches,
   return LB3DC_OK;
 }
 
-int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc) {
+int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc, int split) {
   if (!h) return LB3DC_EINVAL;
   if (h->p.precision != LB3DC_FP32_DEV) return fail(h, LB3DC_ENOTSUP, "launch shape applies to the FP32 path");
   cudaSetDevice(h->device);
-  int rc = fp32_set_shape(h->P, h->s32, FusedShape{tx, ty, zc}, h->stream);
-  return rc ? fail(h, rc, "unsupported launch shape %dx%dx%d", tx, ty, zc) : LB3DC_OK;
+  int rc = fp32_set_shape(h->P, h->s32, FusedShape{tx, ty, zc, split}, h->stream);
+  return rc ? fail(h, rc, "unsupported launch shape %dx%dx%d split %d", tx, ty, zc, split) : LB3DC_OK;
 }
 
-int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc) {
+int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc, int *split) {
   if (!h) return LB3DC_EINVAL;
+  if (split) *split = h->s32.split;
   if (tx) *tx = h->s32.tx;
   if (ty) *ty = h->s32.ty;
   if (zc) *zc = h->s32.zc;

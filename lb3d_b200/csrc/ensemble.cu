@@ -47,7 +47,8 @@ struct lb3dc_ensemble {
   int max_lat = 0, tile_cap = 0, ntiles = 0, grid = 0;
   std::vector<Member> members;
   std::map<long long, long long> free_ranges;  // base -> length
-  FusedShape shape{16, 8, 16};
+  FusedShape shape{16, 8, 16, 1};
+  float4 *M = nullptr, *J = nullptr;
   bool dirty = true;  // tile list must be rebuilt
   bool body = false;
   cudaGraph_t graph = nullptr;
@@ -137,7 +138,7 @@ int rebuild(lb3dc_ensemble *e) {
 cudaError_t launch_step(lb3dc_ensemble *e) {
   cudaError_t r = fp32_launch_fused(e->nc, false, e->body, e->shape, e->d_lat, e->d_tiles, e->ntiles,
                                     e->grid, e->f[0], e->f[1], e->db[0], e->db[1], e->rock, e->S,
-                                    e->stream);
+                                    e->stream, e->M, e->J);
   if (r != cudaSuccess) return r;
   return fp32_flip_parity(e->d_lat, e->max_lat, e->stream);
 }
@@ -263,6 +264,8 @@ int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
     if (ncomp == 3) ok = ok && cudaMalloc(&e->db[b], 3 * (size_t)capacity_sites * 4) == cudaSuccess;
   }
   ok = ok && cudaMalloc(&e->rock, (size_t)capacity_sites) == cudaSuccess;
+  ok = ok && cudaMalloc(&e->M, (size_t)capacity_sites * fp32_moment_bytes(ncomp)) == cudaSuccess;
+  ok = ok && cudaMalloc(&e->J, (size_t)capacity_sites * fp32_own_bytes(ncomp)) == cudaSuccess;
   ok = ok && cudaMalloc(&e->d_lat, (size_t)max_lattices * sizeof(LatDesc)) == cudaSuccess;
   if (!ok) {
     lb3dc_ensemble_destroy(e);
@@ -271,6 +274,7 @@ int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
   cudaMemsetAsync(e->rock, 0, (size_t)capacity_sites, e->stream);
   cudaMemsetAsync(e->d_lat, 0, (size_t)max_lattices * sizeof(LatDesc), e->stream);
   e->bytes = 2 * (long long)pop + (ncomp == 3 ? 24LL * capacity_sites : 0) + capacity_sites +
+             capacity_sites * (fp32_moment_bytes(ncomp) + fp32_own_bytes(ncomp)) +
              (long long)max_lattices * sizeof(LatDesc);
   e->members.resize(max_lattices);
   e->free_ranges[0] = capacity_sites;
@@ -289,6 +293,8 @@ int lb3dc_ensemble_destroy(lb3dc_ensemble *e) {
     if (e->db[b]) cudaFree(e->db[b]);
   }
   if (e->rock) cudaFree(e->rock);
+  if (e->M) cudaFree(e->M);
+  if (e->J) cudaFree(e->J);
   if (e->d_lat) cudaFree(e->d_lat);
   if (e->d_tiles) cudaFree(e->d_tiles);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -303,9 +309,10 @@ int lb3dc_ensemble_last_error(const lb3dc_ensemble *e, char *buf, int len) {
   return LB3DC_OK;
 }
 
-int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc) {
+int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc, int split) {
   if (!e) return LB3DC_EINVAL;
-  FusedShape sh{tx, ty, zc};
+  if (split != 0 && split != 1) return efail(e, LB3DC_EINVAL, "split must be 0 or 1");
+  FusedShape sh{tx, ty, zc, split};
   if (fp32_fused_ctas_per_sm(e->nc, false, false, sh) < 1 || zc < 1)
     return efail(e, LB3DC_EINVAL, "unsupported launch shape");
   e->shape = sh;

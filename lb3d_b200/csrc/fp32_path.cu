@@ -156,28 +156,37 @@ __device__ __forceinline__ int wrap_small(int v, int n) {
   return v < 0 ? v + n : (v >= n ? v - n : v);
 }
 
-template <int NC, int TX, int TY>
+// Kernel modes.  FUSED: one pass per step (moments recomputed on the halo).
+// MOMENTS + COLLIDE: the split strategy, two passes per step: MOMENTS
+// writes each site's post-stream moment entry (the A-ring entry) to a
+// global field M exactly once, COLLIDE loads M with its halo into the same
+// rings and runs the dipole, force and BGK stages.
+constexpr int MODE_FUSED = 0, MODE_MOMENTS = 1, MODE_COLLIDE = 2;
+
+template <int NC, int TX, int TY, int MODE>
 struct FusedGeom {
   static constexpr int NT = TX * TY;
-  static constexpr int H = (NC == 3) ? 2 : 1;
+  static constexpr int H = (MODE == MODE_MOMENTS) ? 0 : ((NC == 3) ? 2 : 1);
   static constexpr int AW = TX + 2 * H, AH = TY + 2 * H, AN = AW * AH;
   static constexpr int AV = (NC == 3) ? 2 : 1;  // float4 per A entry
   static constexpr int AR = (NC == 3) ? 4 : 3;  // A ring depth
   static constexpr int BW = TX + 2, BH = TY + 2, BN = BW * BH;
-  static constexpr int DW = TX + 6, DH = TY + 6, DN = DW * DH;
-  static constexpr int A_F4 = AR * AV * AN;
-  static constexpr int B_F4 = (NC == 3) ? 3 * BN : 0;
-  static constexpr int D_F4 = (NC == 3) ? 3 * DN : 0;
+  static constexpr int DH_ = (MODE == MODE_MOMENTS) ? 1 : 3;  // D-ring halo
+  static constexpr int DW = TX + 2 * DH_, DH = TY + 2 * DH_, DN = DW * DH;
+  static constexpr int A_F4 = (MODE == MODE_MOMENTS) ? 0 : AR * AV * AN;
+  static constexpr int B_F4 = (NC == 3 && MODE != MODE_MOMENTS) ? 3 * BN : 0;
+  static constexpr int D_F4 = (NC == 3 && MODE != MODE_COLLIDE) ? 3 * DN : 0;
   static constexpr int SMEM = 16 * (A_F4 + B_F4 + D_F4);
 };
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY>
-__global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 ? 2 : 3)))
+template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE>
+__global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * TY) : (TX * TY >= 512 ? 1 : (TX * TY >= 256 ? 2 : 3))))
     k_fused(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
-            float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, int S) {
-  using G = FusedGeom<NC, TX, TY>;
+            float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, int S,
+            float4 *__restrict__ Mf, float4 *__restrict__ Jf) {
+  using G = FusedGeom<NC, TX, TY, MODE>;
   constexpr int NT = G::NT, H = G::H, AW = G::AW, AN = G::AN, AV = G::AV, AR = G::AR;
-  constexpr int BW = G::BW, BN = G::BN, DW = G::DW, DN = G::DN;
+  constexpr int BW = G::BW, BN = G::BN, DW = G::DW, DN = G::DN, DHH = G::DH_;
   extern __shared__ float4 smem4[];
   float4 *ringA = smem4;              // [AR][AV][AN]
   float4 *ringB = ringA + G::A_F4;    // [3][BN]
@@ -200,6 +209,8 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
     const int zfirst = z0 - H;
     const int niter = zc + 2 * H;
+    float4 *__restrict__ Mb = Mf ? Mf + base : nullptr;  // moment field of this lattice
+    float4 *__restrict__ Jb = Jf ? Jf + base : nullptr;  // own-site moments
     // halo coordinates stay within one period of the lattice when the
     // lattice is at least a tile plus halo wide; otherwise use modulo
     const bool small = (nx < TX + 3) || (ny < TY + 3);
@@ -210,19 +221,19 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 
       const int gz = pmod(zfirst - 1 + j, nz);
       float4 *dst = ringD + (j % 3) * DN;
       for (int s = tid; s < DN; s += NT) {
-        const int gx = wx(x0 - 3 + s % DW), gy = wy(y0 - 3 + s / DW);
+        const int gx = wx(x0 - DHH + s % DW), gy = wy(y0 - DHH + s / DW);
         const int i = gx + nx * (gy + ny * gz);
         dst[s] = make_float4(__ldg(DBi + i), __ldg(DBi + S + i), __ldg(DBi + 2 * S + i), 0.0f);
       }
     };
-    if (NC == 3) {
+    if (NC == 3 && MODE != MODE_COLLIDE) {
       load_db_plane(0);
       load_db_plane(1);
     }
 
     for (int it = 0; it < niter; ++it) {
       const int zA = zfirst + it;
-      if (NC == 3) load_db_plane(it + 2);
+      if (NC == 3 && MODE != MODE_COLLIDE) load_db_plane(it + 2);
       __syncthreads();
       // ---------------- stage A: post-stream moments on the haloed tile ----
       {
@@ -238,7 +249,7 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 
           Nbr nb;
           make_nbr(nb, gx, gy, gz, nx, ny, nz);
           const int self = noff<18, 1>(nb);
-          float dr[NC];
+          float dr[NC], jm[NC][3];
           float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
@@ -248,6 +259,19 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 
 #pragma unroll
             for (int q = 0; q < 19; ++q) acc = fmaf((float)gw(q), d[q], acc);
             dr[c] = acc;
+            if (MODE == MODE_MOMENTS) {
+              float j0 = 0.f, j1 = 0.f, j2 = 0.f;
+#pragma unroll
+              for (int q = 0; q < 19; ++q) {
+                const float ng = (float)gw(q) * d[q];
+                if (cx(q)) j0 += cx(q) * ng;
+                if (cy(q)) j1 += cy(q) * ng;
+                if (cz(q)) j2 += cz(q) * ng;
+              }
+              jm[c][0] = j0;
+              jm[c][1] = j1;
+              jm[c][2] = j2;
+            }
             if (NC == 3 && c == 2) {
               // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
               // (code/lb3d_advection.F90:137-148)
@@ -263,16 +287,37 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 
               }
             }
           }
+          float4 e0, e1;
           if (NC == 3) {
-            slot[s] = make_float4(dr[1] - dr[0], dr[NC - 1], a0, a1);
-            slot[AN + s] = make_float4(a2, -em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]),
-                                       -em0 * expm1f(-dr[NC - 1]));
+            e0 = make_float4(dr[1] - dr[0], dr[NC - 1], a0, a1);
+            e1 = make_float4(a2, -em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]),
+                             -em0 * expm1f(-dr[NC - 1]));
           } else {
-            slot[s] = make_float4(-em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]), 0.f, 0.f);
+            e0 = make_float4(-em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]), 0.f, 0.f);
+          }
+          if (MODE == MODE_MOMENTS) {
+            // one entry per site, the tile only (H = 0)
+            if (x0 + ax < nx && y0 + ay < ny) {
+              if (NC == 3) {
+                Mb[self] = e0;
+                Mb[S + self] = e1;
+                Jb[self] = make_float4(dr[0], dr[1], dr[2], jm[0][0]);
+                Jb[S + self] = make_float4(jm[0][1], jm[0][2], jm[1][0], jm[1][1]);
+                Jb[2 * S + self] = make_float4(jm[1][2], jm[NC - 1][0], jm[NC - 1][1], jm[NC - 1][2]);
+              } else {
+                reinterpret_cast<float2 *>(Mb)[self] = make_float2(e0.x, e0.y);
+                Jb[self] = make_float4(dr[0], dr[1], jm[0][0], jm[0][1]);
+                Jb[S + self] = make_float4(jm[0][2], jm[1][0], jm[1][1], jm[1][2]);
+              }
+            }
+          } else {
+            slot[s] = e0;
+            if (NC == 3) slot[AN + s] = e1;
           }
         }
-      }
+      }  // stage A
       __syncthreads();
+      if (MODE == MODE_MOMENTS) continue;
       // ---------------- stage B (ternary): dipole relaxation ----------------
       if (NC == 3 && it >= 2) {
         float4 *slotB = ringB + (it % 3) * BN;
@@ -546,6 +591,8 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 512 ? 1 : (TX * TY >= 256 
   }
 }
 
+#include "fp32_split.cuh"
+
 __global__ void k_flip(LatDesc *lats, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && (lats[i].flags & LAT_ACTIVE)) lats[i].parity ^= 1;
@@ -569,30 +616,50 @@ using namespace f32;
 // ---------------------------------------------------------------------------
 // launch table
 // ---------------------------------------------------------------------------
-size_t fp32_fused_smem(int nc, const FusedShape &sh) {
-  const int H = nc == 3 ? 2 : 1;
+constexpr int MODE_DIPOLE = 3;
+
+size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
+  const size_t AN1 = (size_t)(sh.tx + 2) * (sh.ty + 2);
+  if (mode == MODE_DIPOLE) return 16 * 3 * 2 * AN1;
+  if (mode == MODE_COLLIDE) return 16 * 3 * AN1 * (nc == 3 ? 2 : 1);
+  const int H = mode == MODE_MOMENTS ? 0 : (nc == 3 ? 2 : 1);
+  const int dh = mode == MODE_MOMENTS ? 1 : 3;
   const size_t AN = (size_t)(sh.tx + 2 * H) * (sh.ty + 2 * H);
   const size_t BN = (size_t)(sh.tx + 2) * (sh.ty + 2);
-  const size_t DN = (size_t)(sh.tx + 6) * (sh.ty + 6);
-  if (nc == 3) return 16 * (4 * 2 * AN + 3 * BN + 3 * DN);
-  return 16 * (3 * AN);
+  const size_t DN = (size_t)(sh.tx + 2 * dh) * (sh.ty + 2 * dh);
+  size_t f4 = 0;
+  if (mode != MODE_MOMENTS) f4 += (nc == 3 ? 4 * 2 : 3) * AN;
+  if (nc == 3 && mode != MODE_MOMENTS) f4 += 3 * BN;
+  if (nc == 3) f4 += 3 * DN;
+  return 16 * f4;
 }
+size_t fp32_fused_smem(int nc, const FusedShape &sh) { return fp32_mode_smem(nc, sh, MODE_FUSED); }
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE>
 static const void *fused_ptr() {
-  return (const void *)k_fused<NC, TX, TY, ROCK, BODY>;
+  if constexpr (MODE == MODE_COLLIDE)
+    return (const void *)k_split_collide<NC, TX, TY, ROCK, BODY>;
+  else if constexpr (MODE == MODE_DIPOLE)
+    return (const void *)k_split_dipole<TX, TY>;
+  else
+    return (const void *)k_fused<NC, TX, TY, ROCK, BODY, MODE>;
 }
 
-static const void *fused_fn(int nc, bool rock, bool body, const FusedShape &sh) {
-#define LB3D_SHAPES(NC, R, B)                                                  \
-  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B>();          \
-  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B>();          \
-  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B>();        \
-  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B>();          \
-  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B>();
+template <int MODE>
+static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
+#define LB3D_SHAPES(NC, R, B)                                                       \
+  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B, MODE>();         \
+  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B, MODE>();         \
+  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B, MODE>();       \
+  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B, MODE>();         \
+  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B, MODE>();
+  // the moments and dipole passes do not apply the body force
+  if (MODE == MODE_MOMENTS || MODE == MODE_DIPOLE) body = false;
+  if (MODE == MODE_DIPOLE) rock = false;
   if (nc == 3) {
     if (body) { LB3D_SHAPES(3, false, true) } else { LB3D_SHAPES(3, false, false) }
   } else {
+    if (MODE == MODE_DIPOLE) return nullptr;
     if (rock) {
       if (body) { LB3D_SHAPES(2, true, true) } else { LB3D_SHAPES(2, true, false) }
     } else {
@@ -603,10 +670,20 @@ static const void *fused_fn(int nc, bool rock, bool body, const FusedShape &sh) 
   return nullptr;
 }
 
-int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh) {
-  const void *fn = fused_fn(nc, rock, body, sh);
+static const void *kernel_fn(int nc, bool rock, bool body, const FusedShape &sh, int mode) {
+  if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS>(nc, rock, body, sh);
+  if (mode == MODE_COLLIDE) return mode_fn<MODE_COLLIDE>(nc, rock, body, sh);
+  if (mode == MODE_DIPOLE) return mode_fn<MODE_DIPOLE>(nc, rock, body, sh);
+  return mode_fn<MODE_FUSED>(nc, rock, body, sh);
+}
+static const void *fused_fn(int nc, bool rock, bool body, const FusedShape &sh) {
+  return kernel_fn(nc, rock, body, sh, MODE_FUSED);
+}
+
+static int mode_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh, int mode) {
+  const void *fn = kernel_fn(nc, rock, body, sh, mode);
   if (!fn) return 0;
-  size_t smem = fp32_fused_smem(nc, sh);
+  size_t smem = fp32_mode_smem(nc, sh, mode);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return 0;
   int n = 0;
@@ -614,20 +691,58 @@ int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh) {
   return n;
 }
 
+int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh) {
+  int a = mode_ctas_per_sm(nc, rock, body, sh, sh.split ? MODE_COLLIDE : MODE_FUSED);
+  if (!sh.split) return a;
+  int b = mode_ctas_per_sm(nc, rock, body, sh, MODE_MOMENTS);
+  int c = nc == 3 ? mode_ctas_per_sm(nc, rock, body, sh, MODE_DIPOLE) : b;
+  return std::min(a, std::min(b, c));
+}
+
+static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const FusedShape &sh,
+                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
+                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
+                               int S, float4 *M, float4 *J, cudaStream_t st) {
+  const void *fn = kernel_fn(nc, rock, body, sh, mode);
+  if (!fn) return cudaErrorInvalidConfiguration;
+  size_t smem = fp32_mode_smem(nc, sh, mode);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (mode == MODE_DIPOLE) {
+    const float4 *Mc = M;
+    void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&db0, (void *)&db1,
+                    (void *)&Mc, (void *)&S};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
+  }
+  if (mode == MODE_COLLIDE) {
+    const float4 *Mc = M, *Jc = J;
+    void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&f0, (void *)&f1,
+                    (void *)&db0, (void *)&db1, (void *)&rockp, (void *)&S, (void *)&Mc, (void *)&Jc};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
+  }
+  void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&f0, (void *)&f1,
+                  (void *)&db0, (void *)&db1, (void *)&rockp, (void *)&S, (void *)&M, (void *)&J};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
+}
+
 cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
-                              long long S64, cudaStream_t st) {
-  const void *fn = fused_fn(nc, rock, body, sh);
+                              long long S64, cudaStream_t st, float4 *M, float4 *J) {
   if (S64 * 19 * nc >= (1LL << 31)) return cudaErrorInvalidValue;
-  int S = (int)S64;
-  if (!fn) return cudaErrorInvalidConfiguration;
-  size_t smem = fp32_fused_smem(nc, sh);
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int S = (int)S64;
+  if (!sh.split)
+    return launch_mode(MODE_FUSED, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0, f1, db0,
+                       db1, rockp, S, nullptr, nullptr, st);
+  if (!M || !J) return cudaErrorInvalidValue;
+  cudaError_t e = launch_mode(MODE_MOMENTS, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0,
+                              f1, db0, db1, rockp, S, M, J, st);
+  if (e == cudaSuccess && nc == 3)
+    e = launch_mode(MODE_DIPOLE, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0, f1, db0,
+                    db1, rockp, S, M, J, st);
   if (e != cudaSuccess) return e;
-  void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&f0, (void *)&f1,
-                  (void *)&db0, (void *)&db1, (void *)&rockp, (void *)&S};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
+  return launch_mode(MODE_COLLIDE, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0, f1, db0,
+                     db1, rockp, S, M, J, st);
 }
 
 cudaError_t fp32_flip_parity(LatDesc *d_lat, int nlat, cudaStream_t st) {
@@ -696,11 +811,12 @@ LatDesc fp32_make_desc(const DevParams &P, double rho0, long long base, bool roc
 // ---------------------------------------------------------------------------
 long long fp32_footprint(const lb3dc_params &p) {
   const long long N = (long long)p.nx * p.ny * p.nz;
-  return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) + 4096;
+  return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
+         N * (fp32_moment_bytes(p.ncomp) + fp32_own_bytes(p.ncomp)) + 4096;
 }
 
 static FusedShape default_shape(const DevParams &P) {
-  FusedShape sh{32, 8, 16};
+  FusedShape sh{32, 8, 16, P.nc == 3 ? 1 : 0};
   if (P.nx < 32) sh = FusedShape{16, 16, 16};
   if (P.nc == 2) sh.zc = 32;
   return sh;
@@ -719,6 +835,7 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
   s.tx = sh.tx;
   s.ty = sh.ty;
   s.zc = sh.zc;
+  s.split = sh.split;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -731,6 +848,8 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
 
 int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
   if (!fused_fn(P.nc, false, false, sh)) return LB3DC_EINVAL;
+  if (sh.split && !s.M) return LB3DC_EINVAL;
+  if (sh.split != 0 && sh.split != 1) return LB3DC_EINVAL;
   if (sh.zc < 1) return LB3DC_EINVAL;
   return rebuild_tiles(P, s, sh, st);
 }
@@ -743,7 +862,7 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
     if (t[0] > 2 * P.nx && t[0] > 16) continue;
     for (int zc : zcs) {
       if (zc > P.nz && zc != 8) continue;
-      out.push_back(FusedShape{t[0], t[1], zc});
+      for (int split = 0; split < 2; ++split) out.push_back(FusedShape{t[0], t[1], zc, split});
     }
   }
   return out;
@@ -763,7 +882,7 @@ int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double 
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  FusedShape best{s.tx, s.ty, s.zc};
+  FusedShape best{s.tx, s.ty, s.zc, s.split};
   float best_ms = 1e30f;
   KernelTimer *saved_timer = s.timer;
   s.timer = nullptr;
@@ -779,7 +898,7 @@ int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double 
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     ms /= reps;
-    if (ms_out && n < 32) ms_out[n] = ms;
+    if (ms_out && n < 64) ms_out[n] = ms;
     ++n;
     if (ms < best_ms) {
       best_ms = ms;
@@ -815,6 +934,9 @@ int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStre
       cudaMemsetAsync(s.db[b], 0, 3 * N * sizeof(float), st);
     }
   }
+  if (cudaMalloc(&s.M, (size_t)N * fp32_moment_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
+  if (cudaMalloc(&s.J, (size_t)N * fp32_own_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
+  s.bytes += N * (fp32_moment_bytes(P.nc) + fp32_own_bytes(P.nc));
   if (cudaMalloc(&s.d_lat, sizeof(LatDesc)) != cudaSuccess) return LB3DC_ENOMEM;
   s.lat = fp32_make_desc(P, p.rho0 > 0 ? p.rho0 : 0.7, 0, false);
   return rebuild_tiles(P, s, default_shape(P), st);
@@ -828,8 +950,12 @@ void fp32_free(Fp32State &s) {
   }
   if (s.d_lat) cudaFree(s.d_lat);
   if (s.d_tiles) cudaFree(s.d_tiles);
+  if (s.M) cudaFree(s.M);
+  if (s.J) cudaFree(s.J);
   s.d_lat = nullptr;
   s.d_tiles = nullptr;
+  s.M = nullptr;
+  s.J = nullptr;
 }
 
 int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const double *n,
@@ -922,12 +1048,12 @@ int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_
 }
 
 int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st) {
-  FusedShape sh{s.tx, s.ty, s.zc};
+  FusedShape sh{s.tx, s.ty, s.zc, s.split};
   const bool rk = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
   for (int i = 0; i < nsteps; ++i) {
     if (s.timer) s.timer->start(st);
     cudaError_t e = fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, s.grid,
-                                      s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st);
+                                      s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M, s.J);
     if (s.timer) {
       s.timer->stop(st);
       s.timer->launches += 2;

@@ -44,6 +44,9 @@ struct Fp32State {
   LatDesc lat{};        // host copy (single-lattice handle)
   long long S = 0;      // stride (sites)
   int tx = 32, ty = 8, zc = 16;  // launch shape (autotuned)
+  int split = 0;                 // kernel strategy (autotuned)
+  float4 *M = nullptr;           // stencil moment field of the split strategy
+  float4 *J = nullptr;           // own-site densities and momenta (split)
   int grid = 0;
   long long bytes = 0;
   KernelTimer *timer = nullptr;  // optional, owned by the handle
@@ -52,6 +55,7 @@ struct Fp32State {
 // Launch configuration of the fused kernel.
 struct FusedShape {
   int tx, ty, zc;
+  int split = 0;  // 0: one fused pass per step; 1: moments pass + collide pass
 };
 
 long long fp32_footprint(const lb3dc_params &p);
@@ -79,7 +83,11 @@ void fp32_tiles_for(const LatDesc &L, int lat_id, const FusedShape &sh, std::vec
 cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
-                              long long S, cudaStream_t st);
+                              long long S, cudaStream_t st, float4 *M = nullptr,
+                              float4 *J = nullptr);
+// Bytes per site of the split strategy's moment fields.
+inline long long fp32_moment_bytes(int nc) { return nc == 3 ? 32 : 8; }
+inline long long fp32_own_bytes(int nc) { return nc == 3 ? 48 : 32; }
 // Flips the parity of every active lattice (one tiny kernel).
 cudaError_t fp32_flip_parity(LatDesc *d_lat, int nlat, cudaStream_t st);
 size_t fp32_fused_smem(int nc, const FusedShape &sh);

@@ -1,0 +1,343 @@
+// fp32_split.cuh -- the split strategy of the FP32 deviation path, included
+// by fp32_path.cu after its helpers.
+//
+// Per step, three passes over the tile list:
+//   moments (k_fused in MODE_MOMENTS): post-stream moments of every site once,
+//       written as the moment field M (the stencil inputs: rho_b - rho_r,
+//       drho_s, da, psi deviations) and J (the own-site densities and
+//       momenta the BGK update needs);
+//   dipole  (k_split_dipole, ternary): new dipoles on each tile from M with a
+//       one-site halo, code/lb3d_collision.F90:296-403;
+//   collide (k_split_collide): Shan-Chen force from M and the new dipoles
+//       with a one-site halo, body force, one pull of the own populations,
+//       BGK, store.
+// Each pass reads its stencil field through a three-plane ring in shared
+// memory while marching in z, so every field is loaded from global memory
+// once per tile plane (halos hit L2).
+
+// Dipole relaxation of one site from the moment ring planes (entries
+// e0 = {rho_b - rho_r, drho_s, da_x, da_y}, e1 = {da_z, ...} at
+// [plane][0][i] and [plane][AN + i]).
+template <int AW, int AN>
+__device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0, const float4 *Ap,
+                                              int as, const LatDesc &Lg, float rho0) {
+  const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
+  const float4 own0 = A0[as];
+  const float own_daz = A0[AN + as].x;
+  float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
+  float hs0 = own0.z, hs1 = own0.w, hs2 = own_daz;
+  const float isN = 1.0f / fmaxf(rho0 + own0.y, 1.0e-4f);
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
+    const int an = as + cx(q) + AW * cy(q);
+    const float4 e0 = Aq[an];
+    const float pz = Aq[AN + an].x;
+    const float g = (float)gw(q);
+    const float hcm = -sgn * e0.x * g;
+    const float dot2 = 2.0f * (cx(q) * e0.z + cy(q) * e0.w + cz(q) * pz);
+    if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
+    if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
+    if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
+    hs0 = fmaf(e0.z - cx(q) * dot2, g, hs0);
+    hs1 = fmaf(e0.w - cy(q) * dot2, g, hs1);
+    hs2 = fmaf(pz - cz(q) * dot2, g, hs2);
+  }
+  const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
+  const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
+  const float hm = Lg.beta * hn;
+  const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
+  const float od = Lg.omega_d, om1 = (1.0f - od) * isN;
+  return make_float3(od * fac * h0 + om1 * own0.z, od * fac * h1 + om1 * own0.w,
+                     od * fac * h2 + om1 * own_daz);
+}
+
+// Ternary Shan-Chen force (code/lb3d_force_shanchen.F90:215-330) of one
+// site from psi entries P = {-, dpsi_r, dpsi_b, dpsi_s} and dipole entries B
+// (stride W in both), accumulated as neighbour moments so that the own
+// dipole d enters once:
+//   f_cs = SA - 2V, f_sc = SG d - 2 T d, f_ss = M^T d + M d + tr(M) d - 2 Q d
+// with a = d(y) psi_s(y), SA = sum g a, V = sum g (a.c) c, G = g (psi_b -
+// psi_r), SG = sum G, T = sum G c c^T, M = sum 8g a c^T, Q = sum 8g (a.c) c c^T.
+template <int W>
+__device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0, const float4 *Pp,
+                                              const float4 *Bm, const float4 *B0, const float4 *Bp,
+                                              int as, const LatDesc &Lg, float psi0, float Fx[3][3]) {
+  float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, SA[3] = {0, 0, 0}, V[3] = {0, 0, 0};
+  float SG = 0.f, T[6] = {0, 0, 0, 0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0};
+  float M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    const float4 *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
+    const float4 *Bq = cz(q) == 1 ? Bp : (cz(q) == -1 ? Bm : B0);
+    const int an = as + cx(q) + W * cy(q);
+    const float g = (float)gw(q);
+    const int c[3] = {cx(q), cy(q), cz(q)};
+    const float4 e = Pq[an];
+    const float4 b = Bq[an];
+    const float ps = psi0 + e.w;
+    const float a[3] = {b.x * ps, b.y * ps, b.z * ps};
+    float ac = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (c[k]) ac = fmaf((float)c[k], a[k], ac);
+    const float Gq = g * (e.z - e.y);
+    const float g8 = 8.0f * g;
+    SG += Gq;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      SA[k] = fmaf(g, a[k], SA[k]);
+      if (c[k]) {
+        frb[k] = fmaf(g * (float)c[k], e.z, frb[k]);
+        fbr[k] = fmaf(g * (float)c[k], e.y, fbr[k]);
+        V[k] = fmaf(g * (float)c[k], ac, V[k]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) M[i][k] = fmaf(g8 * (float)c[k], a[i], M[i][k]);
+      }
+    }
+#define LB3D_SYM(I, J, K)                  \
+  if (c[I] && c[J]) {                      \
+    const float cc = (float)(c[I] * c[J]); \
+    T[K] = fmaf(Gq, cc, T[K]);             \
+    Q[K] = fmaf(g8 * ac, cc, Q[K]);        \
+  }
+    LB3D_SYM(0, 0, 0) LB3D_SYM(1, 1, 1) LB3D_SYM(2, 2, 2)
+    LB3D_SYM(0, 1, 3) LB3D_SYM(0, 2, 4) LB3D_SYM(1, 2, 5)
+#undef LB3D_SYM
+  }
+  const float4 dd = B0[as];
+  const float d[3] = {dd.x, dd.y, dd.z};
+  const float4 own = P0[as];
+  const float psr = psi0 + own.y, psb = psi0 + own.z, pss = psi0 + own.w;
+  const float Td[3] = {T[0] * d[0] + T[3] * d[1] + T[4] * d[2], T[3] * d[0] + T[1] * d[1] + T[5] * d[2],
+                       T[4] * d[0] + T[5] * d[1] + T[2] * d[2]};
+  const float Qd[3] = {Q[0] * d[0] + Q[3] * d[1] + Q[4] * d[2], Q[3] * d[0] + Q[1] * d[1] + Q[5] * d[2],
+                       Q[4] * d[0] + Q[5] * d[1] + Q[2] * d[2]};
+  const float trM = M[0][0] + M[1][1] + M[2][2];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float MTd = M[0][k] * d[0] + M[1][k] * d[1] + M[2][k] * d[2];
+    const float Md = M[k][0] * d[0] + M[k][1] * d[1] + M[k][2] * d[2];
+    const float fcs = SA[k] - 2.0f * V[k];
+    const float fsc = SG * d[k] - 2.0f * Td[k];
+    const float fss = MTd + Md + trM * d[k] - 2.0f * Qd[k];
+    const float cs = -2.0f * Lg.g_bs * fcs;
+    Fx[1][k] = (-Lg.g_br * fbr[k] + cs) * psb;
+    Fx[0][k] = (-Lg.g_br * frb[k] - cs) * psr;
+    Fx[2][k] = (2.0f * Lg.g_bs * fsc - Lg.g_ss * fss) * pss;
+  }
+}
+
+// Binary force with walls (:127-210) from psi entries {dpsi_r, dpsi_b, -, -}.
+template <int W, bool ROCK>
+__device__ __forceinline__ void force_binary(const float4 *Pm, const float4 *P0, const float4 *Pp,
+                                             int as, const Nbr &nb, const uint8_t *__restrict__ RK,
+                                             const LatDesc &Lg, float psi0, float Fx[2][3]) {
+  float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    const float4 *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
+    const int an = as + cx(q) + W * cy(q);
+    const float g = (float)gw(q);
+    const int c[3] = {cx(q), cy(q), cz(q)};
+    bool nrock = false;
+    if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
+    const float4 e = Pq[an];
+    const float pr = nrock ? -psi0 : e.x, pb = nrock ? -psi0 : e.y;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (c[k]) {
+        frb[k] = fmaf(pb * g, (float)c[k], frb[k]);
+        fbr[k] = fmaf(pr * g, (float)c[k], fbr[k]);
+        if (ROCK && nrock) {
+          fwb[k] = fmaf(Lg.psiw_b * g, (float)c[k], fwb[k]);
+          fwr[k] = fmaf(Lg.psiw_r * g, (float)c[k], fwr[k]);
+        }
+      }
+  }
+  const float4 own = P0[as];
+  const float psr = psi0 + own.x, psb = psi0 + own.y;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    Fx[1][k] = (-Lg.g_br * fbr[k] + Lg.wall_b * fwb[k]) * psb;
+    Fx[0][k] = (-Lg.g_br * frb[k] + Lg.wall_r * fwr[k]) * psr;
+  }
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
+    k_split_dipole(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
+                   float *db0, float *db1, const float4 *__restrict__ Mf, int S) {
+  constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2);
+  extern __shared__ float4 sm4[];  // [3][2][AN]
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    const LatDesc &Lg = lats[T.lat];
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    const int base = (int)Lg.base;
+    float *__restrict__ DBo = (Lg.parity ? db0 : db1) + base;
+    const float4 *__restrict__ Mb = Mf + base;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const bool small = (nx < TX + 2) || (ny < TY + 2);
+    for (int it = 0; it < zc + 2; ++it) {
+      const int zA = z0 - 1 + it, gz = pmod(zA, nz);
+      float4 *slot = sm4 + (it % 3) * 2 * AN;
+      for (int s = tid; s < AN; s += NT) {
+        const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
+        const int gx = small ? pmod(vx, nx) : wrap_small(vx, nx);
+        const int gy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        const int i = gx + nx * (gy + ny * gz);
+        slot[s] = __ldg(Mb + i);
+        slot[AN + s] = __ldg(Mb + S + i);
+      }
+      __syncthreads();
+      if (it >= 2) {
+        const int gx = x0 + tx, gy = y0 + ty;
+        if (gx < nx && gy < ny) {
+          const int as = (tx + 1) + AW * (ty + 1);
+          const float3 d = dipole_site<AW, AN>(sm4 + ((it - 2) % 3) * 2 * AN, sm4 + ((it - 1) % 3) * 2 * AN,
+                                                slot, as, Lg, Lg.rho0);
+          const int i = gx + nx * (gy + ny * pmod(zA - 1, nz));
+          DBo[i] = d.x;
+          DBo[S + i] = d.y;
+          DBo[2 * S + i] = d.z;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int NC, int TX, int TY, bool ROCK, bool BODY>
+__global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
+    k_split_collide(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
+                    float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
+                    int S, const float4 *__restrict__ Mf, const float4 *__restrict__ Jf) {
+  constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2);
+  constexpr int JV = (NC == 3) ? 3 : 2;
+  extern __shared__ float4 sm4[];  // psi ring [3][AN], dipole ring [3][AN] (ternary)
+  float4 *ringP = sm4;
+  float4 *ringB = sm4 + 3 * AN;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    const LatDesc &Lg = lats[T.lat];
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    const int base = (int)Lg.base;
+    const int par = Lg.parity;
+    const float *__restrict__ F = (par ? f1 : f0) + base;
+    float *__restrict__ Fo = (par ? f0 : f1) + base;
+    const float *__restrict__ DBn = (NC == 3) ? (par ? db0 : db1) + base : nullptr;  // new dipoles
+    const float4 *__restrict__ Mb = Mf + base;
+    const float4 *__restrict__ Jb = Jf + base;
+    const uint8_t *__restrict__ RK = rock + base;
+    const float rho0 = Lg.rho0, psi0 = Lg.psi0;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const bool small = (nx < TX + 2) || (ny < TY + 2);
+    for (int it = 0; it < zc + 2; ++it) {
+      const int zA = z0 - 1 + it, gz = pmod(zA, nz);
+      float4 *slotP = ringP + (it % 3) * AN;
+      float4 *slotB = ringB + (it % 3) * AN;
+      for (int s = tid; s < AN; s += NT) {
+        const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
+        const int gx = small ? pmod(vx, nx) : wrap_small(vx, nx);
+        const int gy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        const int i = gx + nx * (gy + ny * gz);
+        if (NC == 3) {
+          slotP[s] = __ldg(Mb + S + i);  // {da_z, dpsi_r, dpsi_b, dpsi_s}
+          slotB[s] = make_float4(__ldg(DBn + i), __ldg(DBn + S + i), __ldg(DBn + 2 * S + i), 0.f);
+        } else {
+          const float2 v = __ldg(reinterpret_cast<const float2 *>(Mb) + i);
+          slotP[s] = make_float4(v.x, v.y, 0.f, 0.f);
+        }
+      }
+      __syncthreads();
+      if (it >= 2) {
+        const int gx = x0 + tx, gy = y0 + ty;
+        if (gx < nx && gy < ny) {
+          const int zC = zA - 1;
+          const int gzc = pmod(zC, nz);
+          Nbr nb;
+          make_nbr(nb, gx, gy, gzc, nx, ny, nz);
+          const int self = noff<18, 1>(nb);
+          bool own_rock = false;
+          if (ROCK) own_rock = __ldg(RK + self) != 0;
+          if (!own_rock) {
+            const int as = (tx + 1) + AW * (ty + 1);
+            const float4 *Pm = ringP + ((it - 2) % 3) * AN, *P0 = ringP + ((it - 1) % 3) * AN;
+            float Fx[NC][3];
+            if (NC == 3)
+              force_ternary<AW>(Pm, P0, slotP, ringB + ((it - 2) % 3) * AN, ringB + ((it - 1) % 3) * AN,
+                                slotB, as, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
+            else
+              force_binary<AW, ROCK>(Pm, P0, slotP, as, nb, RK, Lg, psi0,
+                                     reinterpret_cast<float(*)[3]>(Fx));
+            // own densities and momenta from the moments pass
+            float J[4 * JV];
+#pragma unroll
+            for (int v = 0; v < JV; ++v) {
+              const float4 w = __ldg(Jb + v * S + self);
+              J[4 * v] = w.x;
+              J[4 * v + 1] = w.y;
+              J[4 * v + 2] = w.z;
+              J[4 * v + 3] = w.w;
+            }
+            float dr[NC], rho[NC], j[NC][3];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              dr[c] = J[c];
+              rho[c] = rho0 + dr[c];
+              j[c][0] = J[NC + 3 * c];
+              j[c][1] = J[NC + 3 * c + 1];
+              j[c][2] = J[NC + 3 * c + 2];
+            }
+            if (BODY) {
+              const int x1 = gx + 1, y1 = gy + 1, z1 = gzc + 1;
+              bool on;
+              if (Lg.inv_fluid == 9)
+                on = (z1 == 1) || (z1 == nz);
+              else if (Lg.inv_fluid == 20 || Lg.inv_fluid == 21)
+                on = z1 == 1;
+              else
+                on = z1 >= Lg.amin_z && z1 <= Lg.amax_z && x1 >= Lg.amin_x && x1 <= Lg.amax_x &&
+                     y1 >= Lg.amin_y && y1 <= Lg.amax_y;
+              if (on) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                  const float m = Lg.amass[c] * rho[c];
+                  Fx[c][0] = fmaf(m, Lg.g_accn_x, Fx[c][0]);
+                  Fx[c][1] = fmaf(m, Lg.g_accn_y, Fx[c][1]);
+                  Fx[c][2] = fmaf(m, Lg.g_accn, Fx[c][2]);
+                }
+              }
+            }
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f, rt = 0.f;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const float am = Lg.amass[c] * Lg.omega[c];
+              p0 = fmaf(am, j[c][0], p0);
+              p1 = fmaf(am, j[c][1], p1);
+              p2 = fmaf(am, j[c][2], p2);
+              rt = fmaf(am, rho[c], rt);
+            }
+            const float irt = 1.0f / fmaxf(rt, 1.0e-8f);
+            const float u0 = p0 * irt, u1 = p1 * irt, u2 = p2 * irt;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const float k = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
+              float d[19];
+              pull_comp<ROCK, true>(F, S, c, nb, self, RK, d);
+              bgk_update(d, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
+                         fmaf(k, Fx[c][2], u2), Lg.omega[c]);
+              float *fo = Fo + c * 19 * S + self;
+#pragma unroll
+              for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}

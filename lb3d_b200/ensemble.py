@@ -37,7 +37,7 @@ def _bind():
         "lb3dc_ensemble_create": (I, [I, LL, I, ctypes.POINTER(V)]),
         "lb3dc_ensemble_destroy": (I, [V]),
         "lb3dc_ensemble_last_error": (I, [V, ctypes.c_char_p, I]),
-        "lb3dc_ensemble_set_shape": (I, [V, I, I, I]),
+        "lb3dc_ensemble_set_shape": (I, [V, I, I, I, I]),
         "lb3dc_ensemble_admit": (I, [V, P, _D, _D, I, ctypes.POINTER(I)]),
         "lb3dc_ensemble_admit_seeded": (I, [V, P, ctypes.c_ulonglong, _D, ctypes.c_double, I,
                                             ctypes.POINTER(I)]),
@@ -64,7 +64,7 @@ def member_bytes(p: Params) -> int:
 
 
 class Ensemble:
-    def __init__(self, ncomp=3, capacity_sites=1 << 24, max_lattices=1024, shape=(16, 8, 16)):
+    def __init__(self, ncomp=3, capacity_sites=1 << 24, max_lattices=1024, shape=(16, 8, 16, 1)):
         L = _bind()
         h = ctypes.c_void_p()
         rc = L.lb3dc_ensemble_create(int(ncomp), int(capacity_sites), int(max_lattices), ctypes.byref(h))
@@ -76,7 +76,8 @@ class Ensemble:
         self.ncomp = ncomp
         self.capacity = capacity_sites
         if shape:
-            self._ck(L.lb3dc_ensemble_set_shape(self.h, *map(int, shape)))
+            sh = tuple(shape) + ((1,) if len(shape) == 3 else ())
+            self._ck(L.lb3dc_ensemble_set_shape(self.h, *map(int, sh)))
 
     def _err(self):
         buf = ctypes.create_string_buffer(512)

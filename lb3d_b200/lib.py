@@ -70,8 +70,9 @@ def lib():
         "lb3dc_collision": (I, [H]),
         "lb3dc_time_loop": (I, [H, I]),
         "lb3dc_sync": (I, [H]),
-        "lb3dc_set_launch_shape": (I, [H, I, I, I]),
-        "lb3dc_get_launch_shape": (I, [H, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "lb3dc_set_launch_shape": (I, [H, I, I, I, I]),
+        "lb3dc_get_launch_shape": (I, [H, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I),
+                                       ctypes.POINTER(I)]),
         "lb3dc_autotune": (I, [H, _D, ctypes.POINTER(I)]),
         "lb3dc_stream": (ctypes.c_void_p, [H]),
         "lb3dc_set_profiling": (I, [H, I]),
@@ -218,17 +219,18 @@ class Lattice:
         self._ck(lib().lb3dc_sync(self.h))
 
     # -- FP32 launch shape ------------------------------------------------
-    def set_launch_shape(self, tx, ty, zc):
-        self._ck(lib().lb3dc_set_launch_shape(self.h, int(tx), int(ty), int(zc)))
+    def set_launch_shape(self, tx, ty, zc, split=0):
+        self._ck(lib().lb3dc_set_launch_shape(self.h, int(tx), int(ty), int(zc), int(split)))
 
     @property
     def launch_shape(self):
-        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        self._ck(lib().lb3dc_get_launch_shape(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
-        return a.value, b.value, c.value
+        a, b, c, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().lb3dc_get_launch_shape(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                              ctypes.byref(d)))
+        return a.value, b.value, c.value, d.value
 
     def autotune(self):
-        ms = np.zeros(32)
+        ms = np.zeros(64)
         n = ctypes.c_int()
         self._ck(lib().lb3dc_autotune(self.h, ptr(ms), ctypes.byref(n)))
         return self.launch_shape, ms[: n.value].tolist()
