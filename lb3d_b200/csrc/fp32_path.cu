@@ -609,6 +609,18 @@ __global__ void k_to_fp64(const float *__restrict__ f, double *__restrict__ n, l
           (double)f[((long long)c * 19 + q) * S + base + i] + (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
 }
 
+// FP64 populations -> FP32 deviations (upload); rock sites keep n = 0.
+__global__ void k_from_fp64(const double *__restrict__ n, float *__restrict__ f, long long S,
+                            long long base, long long N, int nc, double rho0) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int c = 0; c < nc; ++c)
+    for (int q = 0; q < 19; ++q) {
+      const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+      f[((long long)c * 19 + q) * S + base + i] = (float)(n[((long long)c * 19 + q) * N + i] - w);
+    }
+}
+
 }  // namespace f32
 
 using namespace f32;
@@ -962,13 +974,6 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
                 const double *db, const uint8_t *rockp, cudaStream_t st) {
   const long long N = P.nsites;
   const double rho0 = s.lat.rho0;
-  std::vector<float> h((size_t)P.nc * 19 * N);
-  for (int c = 0; c < P.nc; ++c)
-    for (int q = 0; q < 19; ++q) {
-      const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * (double)rho0;
-      for (long long i = 0; i < N; ++i)
-        h[((size_t)c * 19 + q) * N + i] = (float)(n[((size_t)c * 19 + q) * N + i] - w);
-    }
   // rock flag: any rock site present?
   std::vector<uint8_t> rk(N);
   if (cudaMemcpyAsync(rk.data(), rockp, N, cudaMemcpyDeviceToHost, st) != cudaSuccess) return LB3DC_ECUDA;
@@ -976,24 +981,35 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   bool any = false;
   for (long long i = 0; i < N; ++i) any |= rk[i] != 0;
   if (any && P.nc == 3) return LB3DC_EINVAL;
-  int parity = 0;
   s.lat = fp32_make_desc(P, rho0, 0, any);
-  s.lat.parity = parity;
-  for (int b = 0; b < 2; ++b) {
-    if (cudaMemcpyAsync(s.f[b], h.data(), h.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
-      return LB3DC_ECUDA;
-    if (P.nc == 3) {
-      std::vector<float> d(3 * N);
-      for (long long i = 0; i < 3 * N; ++i) d[i] = (float)db[i];
+  s.lat.parity = 0;
+  // FP64 staging on the device, converted to deviations by a kernel
+  double *dn = nullptr;
+  const size_t nb = (size_t)P.nc * 19 * N * sizeof(double);
+  if (cudaMalloc(&dn, nb) != cudaSuccess) return LB3DC_ENOMEM;
+  cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, st);
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    k_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dn, s.f[b], s.S, 0, N, P.nc, rho0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(dn);
+  if (e != cudaSuccess) return LB3DC_ECUDA;
+  if (P.nc == 3) {
+    std::vector<float> d(3 * N);
+    for (long long i = 0; i < 3 * N; ++i) d[i] = (float)db[i];
+    for (int b = 0; b < 2; ++b)
       if (cudaMemcpyAsync(s.db[b], d.data(), d.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return LB3DC_ECUDA;
-      cudaStreamSynchronize(st);
-    }
+    cudaStreamSynchronize(st);
   }
   if (cudaMemcpyAsync(s.d_lat, &s.lat, sizeof(LatDesc), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return LB3DC_ECUDA;
-  int rc = rebuild_tiles(P, s, default_shape(P), st);
+  // keep the launch shape chosen so far (set or autotuned); the kernel
+  // variant may change with the rock flag
+  int rc = rebuild_tiles(P, s, FusedShape{s.tx, s.ty, s.zc, s.split}, st);
   if (rc) return rc;
+  (void)p;
   return cudaStreamSynchronize(st) == cudaSuccess ? LB3DC_OK : LB3DC_ECUDA;
 }
 
@@ -1002,43 +1018,66 @@ int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, doubl
   const long long N = P.nsites;
   const int nc = P.nc;
   const int cur = s.lat.parity;
-  std::vector<float> h((size_t)nc * 19 * N);
-  if (cudaMemcpyAsync(h.data(), s.f[cur], h.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    return LB3DC_ECUDA;
-  std::vector<float> d(nc == 3 ? 3 * N : 0);
-  if (nc == 3 && cudaMemcpyAsync(d.data(), s.db[cur], d.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    return LB3DC_ECUDA;
-  std::vector<uint8_t> rk(N, 0);
-  if (rockp && cudaMemcpyAsync(rk.data(), rockp, N, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    return LB3DC_ECUDA;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return LB3DC_ECUDA;
   const double rho0 = s.lat.rho0;
-  for (long long i = 0; i < N; ++i) {
-    for (int c = 0; c < nc; ++c) {
-      double r = 0, m0 = 0, m1 = 0, m2 = 0;
-      for (int q = 0; q < 19; ++q) {
-        const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
-        // rock sites hold no populations (code/lb3d_ic_rock.F90:163-170)
-        const double v = rk[i] ? 0.0 : (double)h[((size_t)c * 19 + q) * N + i] + w;
-        if (n) n[((size_t)c * 19 + q) * N + i] = v;
-        const double ng = v * gw(q);
-        r += ng;
-        m0 += ng * cx(q);
-        m1 += ng * cy(q);
-        m2 += ng * cz(q);
+  std::vector<double> tmp;
+  double *nn = n;
+  if (!nn && (rho || mom)) {
+    tmp.resize((size_t)nc * 19 * N);
+    nn = tmp.data();
+  }
+  if (nn) {
+    // deviations -> FP64 populations on the device, one copy back
+    double *dn = nullptr;
+    const size_t nb = (size_t)nc * 19 * N * sizeof(double);
+    if (cudaMalloc(&dn, nb) != cudaSuccess) return LB3DC_ENOMEM;
+    k_to_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.f[cur], dn, s.S, 0, N, nc, rho0);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nn, dn, nb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(dn);
+    if (e != cudaSuccess) return LB3DC_ECUDA;
+  }
+  std::vector<uint8_t> rk(N, 0);
+  if (rockp && (s.lat.flags & LAT_ROCK)) {
+    if (cudaMemcpyAsync(rk.data(), rockp, N, cudaMemcpyDeviceToHost, st) != cudaSuccess) return LB3DC_ECUDA;
+    cudaStreamSynchronize(st);
+    // rock sites hold no populations (code/lb3d_ic_rock.F90:163-170)
+    if (nn)
+      for (long long i = 0; i < N; ++i)
+        if (rk[i])
+          for (int cq = 0; cq < nc * 19; ++cq) nn[(size_t)cq * N + i] = 0.0;
+  }
+  if (rho || mom) {
+    for (int c = 0; c < nc; ++c)
+      for (long long i = 0; i < N; ++i) {
+        double r = 0, m0 = 0, m1 = 0, m2 = 0;
+        for (int q = 0; q < 19; ++q) {
+          const double ng = nn[((size_t)c * 19 + q) * N + i] * gw(q);
+          r += ng;
+          m0 += ng * cx(q);
+          m1 += ng * cy(q);
+          m2 += ng * cz(q);
+        }
+        if (rho) rho[(size_t)c * N + i] = r;
+        if (mom) {
+          mom[((size_t)c * 3 + 0) * N + i] = m0;
+          mom[((size_t)c * 3 + 1) * N + i] = m1;
+          mom[((size_t)c * 3 + 2) * N + i] = m2;
+        }
       }
-      if (rho) rho[(size_t)c * N + i] = r;
-      if (mom) {
-        mom[((size_t)c * 3 + 0) * N + i] = m0;
-        mom[((size_t)c * 3 + 1) * N + i] = m1;
-        mom[((size_t)c * 3 + 2) * N + i] = m2;
-      }
-    }
-    for (int k = 0; k < 3; ++k) {
-      if (db) db[(size_t)k * N + i] = nc == 3 ? (double)d[(size_t)k * N + i] : 0.0;
-      if (da) da[(size_t)k * N + i] = 0.0;
+  }
+  if (db) {
+    if (nc == 3) {
+      std::vector<float> d(3 * N);
+      if (cudaMemcpyAsync(d.data(), s.db[cur], d.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return LB3DC_ECUDA;
+      cudaStreamSynchronize(st);
+      for (long long i = 0; i < 3 * N; ++i) db[i] = d[i];
+    } else {
+      std::memset(db, 0, 3 * N * sizeof(double));
     }
   }
+  if (da) std::memset(da, 0, 3 * N * sizeof(double));
   (void)p;
   return LB3DC_OK;
 }

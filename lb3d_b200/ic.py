@@ -69,45 +69,56 @@ def unit_dipoles(seed, shape):
     return np.stack([r * np.cos(phi), r * np.sin(phi), z])
 
 
-def sphere_pack(nx, ny, nz, seed=1, porosity=0.4, rmin=6, rmax=12, max_tries=200000):
-    """Rock mask [nz][ny][nx] (1 = rock) from seeded random non-overlapping
-    spheres of radius rmin..rmax, placed by rejection (periodic distance)
-    until the void fraction drops to `porosity` or no sphere fits."""
+def sphere_pack(nx, ny, nz, seed=1, porosity=0.4, rmin=6, rmax=12, overlap=False, max_tries=400000):
+    """Rock mask [nz][ny][nx] (1 = rock) from seeded random spheres of radius
+    rmin..rmax (periodic distances), added until the void fraction drops to
+    `porosity` or `max_tries` candidates were drawn.  With overlap=False a
+    candidate overlapping an earlier sphere is rejected (random sequential
+    addition, which jams near a solid fraction of 0.38); overlap=True keeps
+    every candidate, so any porosity is reachable."""
     rock = np.zeros((nz, ny, nx), dtype=np.uint8)
     target = (1.0 - porosity) * nx * ny * nz
-    centres = []
     u = uniform01(seed, 21, 4 * max_tries).reshape(max_tries, 4)
-    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cen = np.zeros((0, 4))
     filled = 0
+    dims = np.array([nx, ny, nz], dtype=np.float64)
     for t in range(max_tries):
         if filled >= target:
             break
-        cx, cy, cz = u[t, 0] * nx, u[t, 1] * ny, u[t, 2] * nz
+        c = u[t, :3] * dims
         r = rmin + u[t, 3] * (rmax - rmin)
-        ok = True
-        for (ox, oy, oz, orad) in centres:
-            dx = min(abs(cx - ox), nx - abs(cx - ox))
-            dy = min(abs(cy - oy), ny - abs(cy - oy))
-            dz = min(abs(cz - oz), nz - abs(cz - oz))
-            if dx * dx + dy * dy + dz * dz < (r + orad) ** 2:
-                ok = False
-                break
-        if not ok:
-            continue
-        centres.append((cx, cy, cz, r))
-        x0, x1 = int(np.floor(cx - r)), int(np.ceil(cx + r)) + 1
-        y0, y1 = int(np.floor(cy - r)), int(np.ceil(cy + r)) + 1
-        z0, z1 = int(np.floor(cz - r)), int(np.ceil(cz + r)) + 1
-        xs = np.arange(x0, x1) % nx
-        ys = np.arange(y0, y1) % ny
-        zs = np.arange(z0, z1) % nz
-        dx = (np.arange(x0, x1) + 0.5 - cx)[None, None, :]
-        dy = (np.arange(y0, y1) + 0.5 - cy)[None, :, None]
-        dz = (np.arange(z0, z1) + 0.5 - cz)[:, None, None]
+        if not overlap and len(cen):
+            d = np.abs(cen[:, :3] - c)
+            d = np.minimum(d, dims - d)
+            if np.any((d * d).sum(1) < (cen[:, 3] + r) ** 2):
+                continue
+        cen = np.vstack([cen, [c[0], c[1], c[2], r]])
+        x0, x1 = int(np.floor(c[0] - r)), int(np.ceil(c[0] + r)) + 1
+        y0, y1 = int(np.floor(c[1] - r)), int(np.ceil(c[1] + r)) + 1
+        z0, z1 = int(np.floor(c[2] - r)), int(np.ceil(c[2] + r)) + 1
+        xs, ys, zs = np.arange(x0, x1) % nx, np.arange(y0, y1) % ny, np.arange(z0, z1) % nz
+        dx = (np.arange(x0, x1) + 0.5 - c[0])[None, None, :]
+        dy = (np.arange(y0, y1) + 0.5 - c[1])[None, :, None]
+        dz = (np.arange(z0, z1) + 0.5 - c[2])[:, None, None]
         inside = (dx * dx + dy * dy + dz * dz) <= r * r
         sub = rock[np.ix_(zs, ys, xs)]
         filled += int(np.count_nonzero(inside & (sub == 0)))
         sub[inside] = 1
         rock[np.ix_(zs, ys, xs)] = sub
-    del xx, yy, zz
     return rock
+
+
+def invasion_state(nx, ny, nz, rock, seed=1, slab=16, rho=0.7, amp=0.01):
+    """Binary porous-invasion initial state: the first `slab` x-planes filled
+    with red at rho, the rest with blue at rho (each + U(-amp, amp)), zero
+    velocity, no populations at rock sites."""
+    shape = (nz, ny, nx)
+    n = np.zeros((2, 19) + shape)
+    red = np.zeros(shape)
+    red[:, :, :slab] = 1.0
+    r_r = red * (rho + noise(seed, 1, shape, amp))
+    r_b = (1.0 - red) * (rho + noise(seed, 2, shape, amp))
+    n[0] = r_r[None] * W[:, None, None, None]
+    n[1] = r_b[None] * W[:, None, None, None]
+    n[:, :, rock != 0] = 0.0
+    return dict(n=n, db=None, rock=rock.astype(np.float64), shear_sum=0.0)

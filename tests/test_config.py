@@ -46,3 +46,13 @@ def test_lees_edwards_flag_and_validation():
     p.ncomp = 3
     with pytest.raises(ValueError, match="Lees Edwards"):
         p.validate()
+
+
+def test_sphere_pack_porosity_and_determinism():
+    from lb3d_b200.ic import sphere_pack
+    a = sphere_pack(48, 40, 32, seed=3, porosity=0.4, rmin=4, rmax=7, overlap=True)
+    b = sphere_pack(48, 40, 32, seed=3, porosity=0.4, rmin=4, rmax=7, overlap=True)
+    assert (a == b).all()
+    assert abs(1.0 - a.mean() - 0.4) < 0.02
+    c = sphere_pack(48, 40, 32, seed=3, porosity=0.4, rmin=4, rmax=7, overlap=False, max_tries=3000)
+    assert 1.0 - c.mean() > 0.55  # non-overlapping spheres jam well before
