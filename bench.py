@@ -211,8 +211,8 @@ def serving(rank, size, nreq=96, seq_sample=4):
 
 
 def run_configs(args):
-    """--configs: BASELINE configs 1-4 on one GPU, one JSON line each (MLUPS,
-    fraction of the HBM roofline, and for config 2 the FP32-vs-FP64 error
+    """--configs: the four single-lattice workloads on one GPU, one JSON line each (MLUPS,
+    fraction of the HBM roofline, and for ternary 128^3 the FP32-vs-FP64 error
     after 1k and 10k steps)."""
     import torch
     from lb3d_b200.config import Params
@@ -235,13 +235,13 @@ def run_configs(args):
         print(json.dumps(d), flush=True)
 
     phys2 = dict(tau_d=1.0, beta=10.0, d_0=1.0, bdist=2, restore=1, g_br=0.08)
-    # config 1: binary 64^3 FP64, 1000 steps
+    # binary 64^3 FP64, 1000 steps
     p1 = Params(nx=64, ny=64, nz=64, ncomp=2, **phys2).finalize()
     st1 = uniform_mixture(64, 64, 64, 2, seed=1)
     v, _ = mlups(p1, st1, 0, 1000)
-    line({"config": 1, "workload": "binary 64^3 periodic FP64 plain, 1000 steps", "mlups": round(v, 1),
+    line({"case": "binary-64", "workload": "binary 64^3 periodic FP64 plain, 1000 steps", "mlups": round(v, 1),
           "frac": round(v * 1e6 * 608 / 1e9 / peak, 4), "bytes_per_site": 608})
-    # config 2: ternary 128^3, FP64 vs FP32 deviation error after 1k and 10k steps
+    # ternary 128^3, FP64 vs FP32 deviation error after 1k and 10k steps
     p2 = workload_params(precision=0)
     st2 = uniform_mixture(L, L, L, 3, seed=1)
     a = Lattice(p2, precision=0)
@@ -257,21 +257,21 @@ def run_configs(args):
         ra, rb = a.download(), b.download()
         d = np.abs(ra["rho"] - rb["rho"])
         phi_a, phi_b = ra["rho"][0] - ra["rho"][1], rb["rho"][0] - rb["rho"][1]
-        line({"config": 2, "steps": target, "workload": "ternary 128^3, FP32-deviation vs FP64 plain",
+        line({"case": "ternary-128-error", "steps": target, "workload": "ternary 128^3, FP32-deviation vs FP64 plain",
               "max_abs_drho": float(d.max()), "rms_drho": float(np.sqrt((d ** 2).mean())),
               "max_abs_dphi": float(np.abs(phi_a - phi_b).max()),
               "rho_range_fp64": [float(ra["rho"].min()), float(ra["rho"].max())],
               "max_abs_ddb": float(np.abs(ra["db"] - rb["db"]).max())})
     a.close()
     b.close()
-    # config 3: binary Lees-Edwards 256x128x128 (x-planes sheared), shear 0.05
+    # binary Lees-Edwards 256x128x128 (x-planes sheared), shear 0.05
     p3 = Params(nx=256, ny=128, nz=128, ncomp=2, boundary_cond=-1, inv_fluid=5, shear_u=0.05,
                 **phys2).finalize()
     st3 = uniform_mixture(256, 128, 128, 2, seed=3)
     v, _ = mlups(p3, st3, 0, 200)
-    line({"config": 3, "workload": "binary Lees-Edwards 256x128x128 FP64 plain (the FP32 kernels do not "
+    line({"case": "lees-edwards-256x128x128", "workload": "binary Lees-Edwards 256x128x128 FP64 plain (the FP32 kernels do not "
           "implement Lees-Edwards)", "mlups": round(v, 1), "frac": round(v * 1e6 * 608 / 1e9 / peak, 4)})
-    # config 4: binary porous 256^3, body force 1e-5 along x, red inlet slab
+    # binary porous 256^3, body force 1e-5 along x, red inlet slab
     rock = sphere_pack(256, 256, 256, seed=4, porosity=0.4, rmin=6, rmax=12, overlap=True)
     por = 1.0 - float(rock.mean())
     p4 = Params(nx=256, ny=256, nz=256, ncomp=2, g_accn_x=1e-5, **phys2).finalize()
@@ -279,7 +279,7 @@ def run_configs(args):
     v32, shape = mlups(p4, st4, 1, 200, tune=True)
     v64, _ = mlups(p4, st4, 0, 50)
     nf = por
-    line({"config": 4, "workload": "binary porous 256^3 (overlapping spheres r 6..12), body force 1e-5",
+    line({"case": "porous-256", "workload": "binary porous 256^3 (overlapping spheres r 6..12), body force 1e-5",
           "porosity": round(por, 4), "mlups_fp32": round(v32, 1), "mlups_fp64": round(v64, 1),
           "frac_fp32": round(v32 * 1e6 * (304 * nf + 1) / 1e9 / peak, 4), "launch_shape": shape})
 
@@ -293,7 +293,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--requests", type=int, default=96)
-    ap.add_argument("--configs", action="store_true", help="measure BASELINE configs 1-4 instead")
+    ap.add_argument("--configs", action="store_true", help="measure the four single-lattice workloads (binary 64^3 FP64, ternary 128^3 FP32 error, "
+                    "Lees-Edwards 256x128x128, porous 256^3) instead")
     ap.add_argument("--error-steps", type=int, default=10000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

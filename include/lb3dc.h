@@ -139,8 +139,12 @@ int lb3dc_sync(lb3dc_handle *h);
  * item; supported (tx,ty): (32,8) (32,4) (16,16) (16,8) (64,4).  split
  * selects the strategy: 0 = one fused stream-collide pass per step (the
  * moments of the halo are recomputed on chip), 1 = a moments pass writing a
- * per-site moment field (32 B ternary, 8 B binary) and a collide pass that
- * reads it with its halo. */
+ * per-site moment field (32 B ternary, 8 B binary) and own-site moments
+ * (48 B / 32 B), a dipole pass (ternary) and a collide pass that reads them
+ * with their halo, 2 = as 1, but the collide pass stages each site's pulled
+ * populations in shared memory with asynchronous copies one plane ahead
+ * and sums the own moments itself (no own-moment field).  All strategies
+ * give the same result up to FP32 rounding; 1 and 2 agree bit for bit. */
 int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc, int split);
 int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc, int *split);
 /* Times every supported shape and strategy on this lattice (on a saved copy

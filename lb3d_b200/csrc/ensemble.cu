@@ -137,7 +137,7 @@ int rebuild(lb3dc_ensemble *e) {
 // One step of every active lattice: the fused kernel, then the parity flip.
 cudaError_t launch_step(lb3dc_ensemble *e) {
   cudaError_t r = fp32_launch_fused(e->nc, false, e->body, e->shape, e->d_lat, e->d_tiles, e->ntiles,
-                                    e->grid, e->f[0], e->f[1], e->db[0], e->db[1], e->rock, e->S,
+                                    0, e->f[0], e->f[1], e->db[0], e->db[1], e->rock, e->S,
                                     e->stream, e->M, e->J);
   if (r != cudaSuccess) return r;
   return fp32_flip_parity(e->d_lat, e->max_lat, e->stream);
@@ -169,7 +169,8 @@ __global__ void k_seed_state(float *f, float *db, long long S, long long base, l
     const double rho = rb[c] + (uniform01(seed, 1 + c, i) * (2.0 * amp) - amp);
     for (int q = 0; q < 19; ++q) {
       const double w = q == 18 ? 1.0 / 3.0 : 1.0 / 36.0;
-      f[((long long)c * 19 + q) * S + base + i] = (float)(rho * w - w * rho0);
+      // rounded step by step (no contraction), as the host generator computes it
+      f[((long long)c * 19 + q) * S + base + i] = (float)__dsub_rn(__dmul_rn(rho, w), __dmul_rn(w, rho0));
     }
   }
   if (nc == 3) {
@@ -311,7 +312,7 @@ int lb3dc_ensemble_last_error(const lb3dc_ensemble *e, char *buf, int len) {
 
 int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc, int split) {
   if (!e) return LB3DC_EINVAL;
-  if (split != 0 && split != 1) return efail(e, LB3DC_EINVAL, "split must be 0 or 1");
+  if (split < 0 || split > 2) return efail(e, LB3DC_EINVAL, "split must be 0, 1 or 2");
   FusedShape sh{tx, ty, zc, split};
   if (fp32_fused_ctas_per_sm(e->nc, false, false, sh) < 1 || zc < 1)
     return efail(e, LB3DC_EINVAL, "unsupported launch shape");

@@ -25,6 +25,9 @@
 // three-kernel split.  Nothing in the path is a dense contraction, so there
 // are no tensor cores; the roofline is HBM bandwidth.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -145,7 +148,7 @@ __device__ __forceinline__ void pull_comp(const float *__restrict__ F, int S, in
 // which bounds the packed capacity at 19*nc*S < 2^31.
 //
 // On-chip rings (float4 entries, one per site):
-//   A  ternary: {rho_b - rho_r, drho_s, da_x, da_y}, {da_z, dpsi_r, dpsi_b,
+//   A  ternary: {rho_b - rho_r, da_x, da_y, da_z}, {drho_s, dpsi_r, dpsi_b,
 //      dpsi_s} on the tile + 2 halo, 4 planes;  binary: {dpsi_r, dpsi_b, -, -}
 //      on the tile + 1 halo, 3 planes
 //   B  ternary: new dipoles {d_x, d_y, d_z, -} on the tile + 1 halo, 3 planes
@@ -289,8 +292,8 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           }
           float4 e0, e1;
           if (NC == 3) {
-            e0 = make_float4(dr[1] - dr[0], dr[NC - 1], a0, a1);
-            e1 = make_float4(a2, -em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]),
+            e0 = make_float4(dr[1] - dr[0], a0, a1, a2);
+            e1 = make_float4(dr[NC - 1], -em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]),
                              -em0 * expm1f(-dr[NC - 1]));
           } else {
             e0 = make_float4(-em0 * expm1f(-dr[0]), -em0 * expm1f(-dr[1]), 0.f, 0.f);
@@ -301,13 +304,17 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
               if (NC == 3) {
                 Mb[self] = e0;
                 Mb[S + self] = e1;
-                Jb[self] = make_float4(dr[0], dr[1], dr[2], jm[0][0]);
-                Jb[S + self] = make_float4(jm[0][1], jm[0][2], jm[1][0], jm[1][1]);
-                Jb[2 * S + self] = make_float4(jm[1][2], jm[NC - 1][0], jm[NC - 1][1], jm[NC - 1][2]);
+                if (Jb) {
+                  Jb[self] = make_float4(dr[0], dr[1], dr[2], jm[0][0]);
+                  Jb[S + self] = make_float4(jm[0][1], jm[0][2], jm[1][0], jm[1][1]);
+                  Jb[2 * S + self] = make_float4(jm[1][2], jm[NC - 1][0], jm[NC - 1][1], jm[NC - 1][2]);
+                }
               } else {
                 reinterpret_cast<float2 *>(Mb)[self] = make_float2(e0.x, e0.y);
-                Jb[self] = make_float4(dr[0], dr[1], jm[0][0], jm[0][1]);
-                Jb[S + self] = make_float4(jm[0][2], jm[1][0], jm[1][1], jm[1][2]);
+                if (Jb) {
+                  Jb[self] = make_float4(dr[0], dr[1], jm[0][0], jm[0][1]);
+                  Jb[S + self] = make_float4(jm[0][2], jm[1][0], jm[1][1], jm[1][2]);
+                }
               }
             }
           } else {
@@ -329,26 +336,25 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
         for (int s = tid; s < BN; s += NT) {
           const int bx = s % BW, by = s / BW;
           const int as = (bx + 1) + AW * (by + 1);
-          const float4 own0 = A0[as];
-          const float own_daz = A0[AN + as].x;
+          const float4 own0 = A0[as];  // {rho_b - rho_r, da}
+          const float own_drs = A0[AN + as].x;
           float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
-          float hs0 = own0.z, hs1 = own0.w, hs2 = own_daz;
-          const float isN = 1.0f / fmaxf(rho0 + own0.y, 1.0e-4f);
+          float hs0 = own0.y, hs1 = own0.z, hs2 = own0.w;
+          const float isN = 1.0f / fmaxf(rho0 + own_drs, 1.0e-4f);
 #pragma unroll
           for (int q = 0; q < 18; ++q) {
             const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
             const int an = as + cx(q) + AW * cy(q);
             const float4 e0 = Aq[an];
-            const float pz = Aq[AN + an].x;
             const float g = (float)gw(q);
             const float hcm = -sgn * e0.x * g;  // e0.x = rho_b - rho_r
-            const float dot2 = 2.0f * (cx(q) * e0.z + cy(q) * e0.w + cz(q) * pz);
+            const float dot2 = 2.0f * (cx(q) * e0.y + cy(q) * e0.z + cz(q) * e0.w);
             if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
             if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
             if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
-            hs0 = fmaf(e0.z - cx(q) * dot2, g, hs0);
-            hs1 = fmaf(e0.w - cy(q) * dot2, g, hs1);
-            hs2 = fmaf(pz - cz(q) * dot2, g, hs2);
+            hs0 = fmaf(e0.y - cx(q) * dot2, g, hs0);
+            hs1 = fmaf(e0.z - cy(q) * dot2, g, hs1);
+            hs2 = fmaf(e0.w - cz(q) * dot2, g, hs2);
           }
           const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
           const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
@@ -358,9 +364,9 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           // first-order term.
           const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
           const float od = Lg.omega_d, om1 = (1.0f - od) * isN;
-          const float n0 = od * fac * h0 + om1 * own0.z;
-          const float n1 = od * fac * h1 + om1 * own0.w;
-          const float n2 = od * fac * h2 + om1 * own_daz;
+          const float n0 = od * fac * h0 + om1 * own0.y;
+          const float n1 = od * fac * h1 + om1 * own0.z;
+          const float n2 = od * fac * h2 + om1 * own0.w;
           slotB[s] = make_float4(n0, n1, n2, 0.0f);
           if (bx >= 1 && bx <= TX && by >= 1 && by <= TY && zB >= z0 && zB < z0 + zc) {
             const int gx = x0 + bx - 1, gy = y0 + by - 1;
@@ -418,7 +424,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
                 const int bn = bs + cx(q) + BW * cy(q);
                 const float g = (float)gw(q);
                 const int c[3] = {cx(q), cy(q), cz(q)};
-                const float4 e = Aq[AN + an];  // {da_z, dpsi_r, dpsi_b, dpsi_s}
+                const float4 e = Aq[AN + an];  // {drho_s, dpsi_r, dpsi_b, dpsi_s}
                 const float4 b = Bq[bn];
                 const float ps = psi0 + e.w;
                 const float a[3] = {b.x * ps, b.y * ps, b.z * ps};
@@ -599,6 +605,8 @@ __global__ void k_flip(LatDesc *lats, int n) {
 }
 
 // FP32 state -> FP64 populations n = delta + w rho0 (dumps, reductions).
+// The products and sums are rounded separately (no contraction), as the
+// host-side conversions of the ensemble do, so both routes agree bit for bit.
 __global__ void k_to_fp64(const float *__restrict__ f, double *__restrict__ n, long long S,
                           long long base, long long N, int nc, double rho0) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -606,7 +614,8 @@ __global__ void k_to_fp64(const float *__restrict__ f, double *__restrict__ n, l
   for (int c = 0; c < nc; ++c)
     for (int q = 0; q < 19; ++q)
       n[((long long)c * 19 + q) * N + i] =
-          (double)f[((long long)c * 19 + q) * S + base + i] + (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+          __dadd_rn((double)f[((long long)c * 19 + q) * S + base + i],
+                    __dmul_rn(q == 18 ? 1.0 / 3.0 : 1.0 / 36.0, rho0));
 }
 
 // FP64 populations -> FP32 deviations (upload); rock sites keep n = 0.
@@ -616,8 +625,8 @@ __global__ void k_from_fp64(const double *__restrict__ n, float *__restrict__ f,
   if (i >= N) return;
   for (int c = 0; c < nc; ++c)
     for (int q = 0; q < 19; ++q) {
-      const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
-      f[((long long)c * 19 + q) * S + base + i] = (float)(n[((long long)c * 19 + q) * N + i] - w);
+      const double w = __dmul_rn(q == 18 ? 1.0 / 3.0 : 1.0 / 36.0, rho0);
+      f[((long long)c * 19 + q) * S + base + i] = (float)__dsub_rn(n[((long long)c * 19 + q) * N + i], w);
     }
 }
 
@@ -628,11 +637,13 @@ using namespace f32;
 // ---------------------------------------------------------------------------
 // launch table
 // ---------------------------------------------------------------------------
-constexpr int MODE_DIPOLE = 3;
+constexpr int MODE_DIPOLE = 3, MODE_COLLIDE2 = 4;
 
 size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
   const size_t AN1 = (size_t)(sh.tx + 2) * (sh.ty + 2);
-  if (mode == MODE_DIPOLE) return 16 * 3 * 2 * AN1;
+  if (mode == MODE_DIPOLE) return 16 * 5 * AN1 + (size_t)4 * 5 * sh.tx * sh.ty;
+  if (mode == MODE_COLLIDE2)
+    return 5 * AN1 * (nc == 3 ? 32 : 8) + (size_t)19 * nc * sh.tx * sh.ty * 4;
   if (mode == MODE_COLLIDE) return 16 * 3 * AN1 * (nc == 3 ? 2 : 1);
   const int H = mode == MODE_MOMENTS ? 0 : (nc == 3 ? 2 : 1);
   const int dh = mode == MODE_MOMENTS ? 1 : 3;
@@ -651,6 +662,8 @@ template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE>
 static const void *fused_ptr() {
   if constexpr (MODE == MODE_COLLIDE)
     return (const void *)k_split_collide<NC, TX, TY, ROCK, BODY>;
+  else if constexpr (MODE == MODE_COLLIDE2)
+    return (const void *)k_split_collide2<NC, TX, TY, ROCK, BODY>;
   else if constexpr (MODE == MODE_DIPOLE)
     return (const void *)k_split_dipole<TX, TY>;
   else
@@ -686,6 +699,7 @@ static const void *kernel_fn(int nc, bool rock, bool body, const FusedShape &sh,
   if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS>(nc, rock, body, sh);
   if (mode == MODE_COLLIDE) return mode_fn<MODE_COLLIDE>(nc, rock, body, sh);
   if (mode == MODE_DIPOLE) return mode_fn<MODE_DIPOLE>(nc, rock, body, sh);
+  if (mode == MODE_COLLIDE2) return mode_fn<MODE_COLLIDE2>(nc, rock, body, sh);
   return mode_fn<MODE_FUSED>(nc, rock, body, sh);
 }
 static const void *fused_fn(int nc, bool rock, bool body, const FusedShape &sh) {
@@ -704,26 +718,64 @@ static int mode_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh, 
 }
 
 int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh) {
-  int a = mode_ctas_per_sm(nc, rock, body, sh, sh.split ? MODE_COLLIDE : MODE_FUSED);
+  int a = mode_ctas_per_sm(nc, rock, body, sh,
+                           sh.split == 2 ? MODE_COLLIDE2 : (sh.split ? MODE_COLLIDE : MODE_FUSED));
   if (!sh.split) return a;
   int b = mode_ctas_per_sm(nc, rock, body, sh, MODE_MOMENTS);
   int c = nc == 3 ? mode_ctas_per_sm(nc, rock, body, sh, MODE_DIPOLE) : b;
   return std::min(a, std::min(b, c));
 }
 
+// Grid of one pass: as many CTAs as are resident at once (up to the tile
+// count), from the pass's own occupancy, so a pass with a large shared
+// memory stage does not throttle the others.  The dynamic shared memory
+// attribute and the occupancy are set up once per kernel and device.
+static cudaError_t prepare_kernel(const void *fn, int nthreads, size_t smem, int *ctas_total) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void *, size_t, int, int>, int> cache;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const auto key = std::make_tuple(fn, smem, nthreads, dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    *ctas_total = it->second;
+    return cudaSuccess;
+  }
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per = 0, nsm = 148;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, nthreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per < 1) return cudaErrorInvalidConfiguration;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cache[key] = *ctas_total = per * nsm;
+  return cudaSuccess;
+}
+
 static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const FusedShape &sh,
-                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
+                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                                float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
                                int S, float4 *M, float4 *J, cudaStream_t st) {
   const void *fn = kernel_fn(nc, rock, body, sh, mode);
   if (!fn) return cudaErrorInvalidConfiguration;
   size_t smem = fp32_mode_smem(nc, sh, mode);
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int resident = 0;
+  cudaError_t e = prepare_kernel(fn, sh.tx * sh.ty, smem, &resident);
   if (e != cudaSuccess) return e;
+  int grid = std::max(1, std::min(ntiles, resident));
+  if (max_grid > 0) grid = std::min(grid, max_grid);
   if (mode == MODE_DIPOLE) {
     const float4 *Mc = M;
     void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&db0, (void *)&db1,
                     (void *)&Mc, (void *)&S};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
+  }
+  if (mode == MODE_COLLIDE2) {
+    const float4 *Mc = M;
+    void *args[] = {(void *)&d_lat, (void *)&d_tiles, (void *)&ntiles, (void *)&f0, (void *)&f1,
+                    (void *)&db0, (void *)&db1, (void *)&rockp, (void *)&S, (void *)&Mc};
     return cudaLaunchKernel(fn, dim3(grid), dim3(sh.tx * sh.ty), args, smem, st);
   }
   if (mode == MODE_COLLIDE) {
@@ -738,23 +790,25 @@ static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const Fus
 }
 
 cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
-                              const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
+                              const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
                               long long S64, cudaStream_t st, float4 *M, float4 *J) {
   if (S64 * 19 * nc >= (1LL << 31)) return cudaErrorInvalidValue;
   const int S = (int)S64;
   if (!sh.split)
-    return launch_mode(MODE_FUSED, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0, f1, db0,
+    return launch_mode(MODE_FUSED, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1, db0,
                        db1, rockp, S, nullptr, nullptr, st);
-  if (!M || !J) return cudaErrorInvalidValue;
-  cudaError_t e = launch_mode(MODE_MOMENTS, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0,
+  if (!M || (sh.split == 1 && !J)) return cudaErrorInvalidValue;
+  // strategy 2 recomputes the own moments in the collide pass: no J field
+  if (sh.split == 2) J = nullptr;
+  cudaError_t e = launch_mode(MODE_MOMENTS, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0,
                               f1, db0, db1, rockp, S, M, J, st);
   if (e == cudaSuccess && nc == 3)
-    e = launch_mode(MODE_DIPOLE, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0, f1, db0,
+    e = launch_mode(MODE_DIPOLE, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1, db0,
                     db1, rockp, S, M, J, st);
   if (e != cudaSuccess) return e;
-  return launch_mode(MODE_COLLIDE, nc, rock, body, sh, d_lat, d_tiles, ntiles, grid, f0, f1, db0,
-                     db1, rockp, S, M, J, st);
+  return launch_mode(sh.split == 2 ? MODE_COLLIDE2 : MODE_COLLIDE, nc, rock, body, sh, d_lat,
+                     d_tiles, ntiles, max_grid, f0, f1, db0, db1, rockp, S, M, J, st);
 }
 
 cudaError_t fp32_flip_parity(LatDesc *d_lat, int nlat, cudaStream_t st) {
@@ -861,7 +915,7 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
 int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
   if (!fused_fn(P.nc, false, false, sh)) return LB3DC_EINVAL;
   if (sh.split && !s.M) return LB3DC_EINVAL;
-  if (sh.split != 0 && sh.split != 1) return LB3DC_EINVAL;
+  if (sh.split < 0 || sh.split > 2) return LB3DC_EINVAL;
   if (sh.zc < 1) return LB3DC_EINVAL;
   return rebuild_tiles(P, s, sh, st);
 }
@@ -874,7 +928,7 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
     if (t[0] > 2 * P.nx && t[0] > 16) continue;
     for (int zc : zcs) {
       if (zc > P.nz && zc != 8) continue;
-      for (int split = 0; split < 2; ++split) out.push_back(FusedShape{t[0], t[1], zc, split});
+      for (int split = 0; split < 3; ++split) out.push_back(FusedShape{t[0], t[1], zc, split});
     }
   }
   return out;
@@ -1091,7 +1145,7 @@ int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, 
   const bool rk = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
   for (int i = 0; i < nsteps; ++i) {
     if (s.timer) s.timer->start(st);
-    cudaError_t e = fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, s.grid,
+    cudaError_t e = fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, 0,
                                       s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M, s.J);
     if (s.timer) {
       s.timer->stop(st);

@@ -55,7 +55,8 @@ struct Fp32State {
 // Launch configuration of the fused kernel.
 struct FusedShape {
   int tx, ty, zc;
-  int split = 0;  // 0: one fused pass per step; 1: moments pass + collide pass
+  int split = 0;  // 0: one fused pass per step; 1: moments (+ dipole) + collide passes;
+                  // 2: as 1 with the asynchronously staged collide pass (no J field)
 };
 
 long long fp32_footprint(const lb3dc_params &p);
@@ -80,8 +81,10 @@ cudaError_t fp32_sanity_counts(const DevParams &P, Fp32State &s, unsigned long l
 // Shared with the ensemble runtime: tile list for a lattice, fused launch.
 void fp32_tiles_for(const LatDesc &L, int lat_id, const FusedShape &sh, std::vector<Tile> &out);
 // fin/fout select by parity inside the kernel; `flip` is applied by caller.
+// Each pass runs as many CTAs as are resident at once for that kernel (at
+// most ntiles); max_grid > 0 caps that number.
 cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
-                              const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int grid,
+                              const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
                               long long S, cudaStream_t st, float4 *M = nullptr,
                               float4 *J = nullptr);

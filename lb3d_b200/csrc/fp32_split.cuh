@@ -3,9 +3,10 @@
 //
 // Per step, three passes over the tile list:
 //   moments (k_fused in MODE_MOMENTS): post-stream moments of every site once,
-//       written as the moment field M (the stencil inputs: rho_b - rho_r,
-//       drho_s, da, psi deviations) and J (the own-site densities and
-//       momenta the BGK update needs);
+//       written as the moment field M, two float4 per ternary site:
+//       {rho_b - rho_r, da} (the dipole stencil input) and {drho_s, psi
+//       deviations} (the force stencil input), and with strategy 1 also J
+//       (the own-site densities and momenta the BGK update needs);
 //   dipole  (k_split_dipole, ternary): new dipoles on each tile from M with a
 //       one-site halo, code/lb3d_collision.F90:296-403;
 //   collide (k_split_collide): Shan-Chen force from M and the new dipoles
@@ -15,41 +16,38 @@
 // memory while marching in z, so every field is loaded from global memory
 // once per tile plane (halos hit L2).
 
-// Dipole relaxation of one site from the moment ring planes (entries
-// e0 = {rho_b - rho_r, drho_s, da_x, da_y}, e1 = {da_z, ...} at
-// [plane][0][i] and [plane][AN + i]).
-template <int AW, int AN>
+// Dipole relaxation of one site (code/lb3d_collision.F90:296-403) from the
+// ring planes of moment entries {rho_b - rho_r, da_x, da_y, da_z} (row
+// stride AW) and the site's own surfactant density deviation.
+template <int AW>
 __device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0, const float4 *Ap,
-                                              int as, const LatDesc &Lg, float rho0) {
+                                              int as, const LatDesc &Lg, float rho0, float own_drs) {
   const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
   const float4 own0 = A0[as];
-  const float own_daz = A0[AN + as].x;
   float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
-  float hs0 = own0.z, hs1 = own0.w, hs2 = own_daz;
-  const float isN = 1.0f / fmaxf(rho0 + own0.y, 1.0e-4f);
+  float hs0 = own0.y, hs1 = own0.z, hs2 = own0.w;
+  const float isN = 1.0f / fmaxf(rho0 + own_drs, 1.0e-4f);
 #pragma unroll
   for (int q = 0; q < 18; ++q) {
     const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-    const int an = as + cx(q) + AW * cy(q);
-    const float4 e0 = Aq[an];
-    const float pz = Aq[AN + an].x;
+    const float4 e0 = Aq[as + cx(q) + AW * cy(q)];
     const float g = (float)gw(q);
     const float hcm = -sgn * e0.x * g;
-    const float dot2 = 2.0f * (cx(q) * e0.z + cy(q) * e0.w + cz(q) * pz);
+    const float dot2 = 2.0f * (cx(q) * e0.y + cy(q) * e0.z + cz(q) * e0.w);
     if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
     if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
     if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
-    hs0 = fmaf(e0.z - cx(q) * dot2, g, hs0);
-    hs1 = fmaf(e0.w - cy(q) * dot2, g, hs1);
-    hs2 = fmaf(pz - cz(q) * dot2, g, hs2);
+    hs0 = fmaf(e0.y - cx(q) * dot2, g, hs0);
+    hs1 = fmaf(e0.z - cy(q) * dot2, g, hs1);
+    hs2 = fmaf(e0.w - cz(q) * dot2, g, hs2);
   }
   const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
   const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
   const float hm = Lg.beta * hn;
   const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
   const float od = Lg.omega_d, om1 = (1.0f - od) * isN;
-  return make_float3(od * fac * h0 + om1 * own0.z, od * fac * h1 + om1 * own0.w,
-                     od * fac * h2 + om1 * own_daz);
+  return make_float3(od * fac * h0 + om1 * own0.y, od * fac * h1 + om1 * own0.z,
+                     od * fac * h2 + om1 * own0.w);
 }
 
 // Ternary Shan-Chen force (code/lb3d_force_shanchen.F90:215-330) of one
@@ -129,20 +127,20 @@ __device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0
 }
 
 // Binary force with walls (:127-210) from psi entries {dpsi_r, dpsi_b, -, -}.
-template <int W, bool ROCK>
-__device__ __forceinline__ void force_binary(const float4 *Pm, const float4 *P0, const float4 *Pp,
+template <int W, bool ROCK, typename E>
+__device__ __forceinline__ void force_binary(const E *Pm, const E *P0, const E *Pp,
                                              int as, const Nbr &nb, const uint8_t *__restrict__ RK,
                                              const LatDesc &Lg, float psi0, float Fx[2][3]) {
   float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
 #pragma unroll
   for (int q = 0; q < 18; ++q) {
-    const float4 *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
+    const E *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
     const int an = as + cx(q) + W * cy(q);
     const float g = (float)gw(q);
     const int c[3] = {cx(q), cy(q), cz(q)};
     bool nrock = false;
     if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
-    const float4 e = Pq[an];
+    const E e = Pq[an];
     const float pr = nrock ? -psi0 : e.x, pb = nrock ? -psi0 : e.y;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
@@ -155,7 +153,7 @@ __device__ __forceinline__ void force_binary(const float4 *Pm, const float4 *P0,
         }
       }
   }
-  const float4 own = P0[as];
+  const E own = P0[as];
   const float psr = psi0 + own.x, psb = psi0 + own.y;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -164,12 +162,37 @@ __device__ __forceinline__ void force_binary(const float4 *Pm, const float4 *P0,
   }
 }
 
+// Asynchronous copies global -> shared (cp.async, 4/8/16 bytes) in commit
+// groups; a thread waits for its own groups, a barrier then publishes them.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Dipole pass: the {rho_b - rho_r, da} entries of M stream through a
+// five-slot ring, refilled with cp.async three planes ahead of the plane
+// being relaxed (one barrier per plane); each thread also prefetches its own
+// site's drho_s.
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
     k_split_dipole(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                    float *db0, float *db1, const float4 *__restrict__ Mf, int S) {
-  constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2);
-  extern __shared__ float4 sm4[];  // [3][2][AN]
+  constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2), RS = 5;
+  extern __shared__ float4 sm4[];  // ring [RS][AN] float4, own drho_s [RS][NT] float
+  float *owns = reinterpret_cast<float *>(sm4 + RS * AN);
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile T = tiles[t];
@@ -180,32 +203,44 @@ __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
     const float4 *__restrict__ Mb = Mf + base;
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
     const bool small = (nx < TX + 2) || (ny < TY + 2);
-    for (int it = 0; it < zc + 2; ++it) {
-      const int zA = z0 - 1 + it, gz = pmod(zA, nz);
-      float4 *slot = sm4 + (it % 3) * 2 * AN;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool act = gx < nx && gy < ny;
+    // ring index r holds plane z0 - 1 + r in slot r % RS
+    auto load_ring = [&](int r) {
+      const int gz = pmod(z0 - 1 + r, nz);
+      float4 *slot = sm4 + (r % RS) * AN;
       for (int s = tid; s < AN; s += NT) {
         const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
-        const int gx = small ? pmod(vx, nx) : wrap_small(vx, nx);
-        const int gy = small ? pmod(vy, ny) : wrap_small(vy, ny);
-        const int i = gx + nx * (gy + ny * gz);
-        slot[s] = __ldg(Mb + i);
-        slot[AN + s] = __ldg(Mb + S + i);
+        const int ix = small ? pmod(vx, nx) : wrap_small(vx, nx);
+        const int iy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        cp_async16(slot + s, Mb + ix + nx * (iy + ny * gz));
       }
-      __syncthreads();
-      if (it >= 2) {
-        const int gx = x0 + tx, gy = y0 + ty;
-        if (gx < nx && gy < ny) {
-          const int as = (tx + 1) + AW * (ty + 1);
-          const float3 d = dipole_site<AW, AN>(sm4 + ((it - 2) % 3) * 2 * AN, sm4 + ((it - 1) % 3) * 2 * AN,
-                                                slot, as, Lg, Lg.rho0);
-          const int i = gx + nx * (gy + ny * pmod(zA - 1, nz));
-          DBo[i] = d.x;
-          DBo[S + i] = d.y;
-          DBo[2 * S + i] = d.z;
-        }
+      if (act)
+        cp_async4(owns + (r % RS) * NT + tid,
+                  reinterpret_cast<const float *>(Mb + S + gx + nx * (gy + ny * gz)));
+    };
+    load_ring(0);
+    load_ring(1);
+    load_ring(2);
+    cp_async_commit();
+    for (int k = 0; k < zc; ++k) {
+      if (k + 3 <= zc + 1) load_ring(k + 3);
+      cp_async_commit();
+      cp_async_wait<1>();  // ring planes up to k + 2 landed (this thread's copies)
+      __syncthreads();     // ... and everybody's
+      if (act) {
+        const int as = (tx + 1) + AW * (ty + 1);
+        const float3 d = dipole_site<AW>(sm4 + (k % RS) * AN, sm4 + ((k + 1) % RS) * AN,
+                                         sm4 + ((k + 2) % RS) * AN, as, Lg, Lg.rho0,
+                                         owns[((k + 1) % RS) * NT + tid]);
+        const int i = gx + nx * (gy + ny * pmod(z0 + k, nz));
+        DBo[i] = d.x;
+        DBo[S + i] = d.y;
+        DBo[2 * S + i] = d.z;
       }
-      __syncthreads();
     }
+    cp_async_wait<0>();
+    __syncthreads();  // the next tile refills ring slots 0..2
   }
 }
 
@@ -339,5 +374,227 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
       }
       __syncthreads();
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Collide pass with asynchronous staging (split strategy 2).
+//
+// The plain collide pass above is latency bound: each thread has at most one
+// component's 19 pulls in flight, and nothing is in flight while it works
+// through the force stencil.  Here every thread copies the 19*NC pulled
+// deviations of its next site straight into its own shared-memory column
+// with cp.async (no registers held) as soon as the current site's BGK
+// update has read the previous ones, so the copies fly during the barrier,
+// the ring refill and the whole force stencil of the next plane.  The
+// psi/dipole rings are refilled the same way, three planes ahead, in a
+// five-slot ring (one barrier per plane).  The own densities and momenta
+// are summed from the staged values in the order the moments pass uses, so
+// the J field is not needed and the result equals the plain collide pass
+// bit for bit.
+// ---------------------------------------------------------------------------
+// Shared-memory layout of k_split_collide2 (bytes): psi ring [5][AN] float4
+// (float2 for binary), dipole ring [5][AN] float4 (ternary), population
+// stage [19*NC][NT] float.
+template <int NC, int TX, int TY>
+struct Collide2Geom {
+  static constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2), RS = 5;
+  static constexpr int PB = (NC == 3) ? 16 : 8;  // psi entry bytes
+  static constexpr int P_BYTES = RS * AN * PB;
+  static constexpr int B_BYTES = (NC == 3) ? RS * AN * 16 : 0;
+  static constexpr int F_BYTES = 19 * NC * NT * 4;
+  static constexpr int SMEM = P_BYTES + B_BYTES + F_BYTES;
+};
+
+// Issues the pulls of component c of one site into the stage column
+// (stage[q * NT]), with half-way bounce-back when ROCK (as pull_comp).
+template <bool ROCK, int NT>
+__device__ __forceinline__ void pull_async(const float *__restrict__ F, int S, int c, const Nbr &n,
+                                           int self, const uint8_t *__restrict__ rk, float *stage) {
+  const float *fc = F + c * 19 * S;
+  cp_async4(stage + 18 * NT, fc + 18 * S + self);
+#define LB3D_APULL(Q)                                                    \
+  {                                                                      \
+    const int up = noff<Q, -1>(n);                                       \
+    bool uf = true;                                                      \
+    if (ROCK) uf = __ldg(rk + up) == 0;                                  \
+    cp_async4(stage + (Q) * NT, fc + (uf ? Q * S + up : bounce(Q) * S + self)); \
+  }
+  LB3D_APULL(0) LB3D_APULL(1) LB3D_APULL(2) LB3D_APULL(3) LB3D_APULL(4) LB3D_APULL(5)
+  LB3D_APULL(6) LB3D_APULL(7) LB3D_APULL(8) LB3D_APULL(9) LB3D_APULL(10) LB3D_APULL(11)
+  LB3D_APULL(12) LB3D_APULL(13) LB3D_APULL(14) LB3D_APULL(15) LB3D_APULL(16) LB3D_APULL(17)
+#undef LB3D_APULL
+}
+
+template <int NC, int TX, int TY, bool ROCK, bool BODY>
+__global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
+    k_split_collide2(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
+                     float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
+                     int S, const float4 *__restrict__ Mf) {
+  using G = Collide2Geom<NC, TX, TY>;
+  constexpr int NT = G::NT, AW = G::AW, AN = G::AN, RS = G::RS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float4 *ringP4 = reinterpret_cast<float4 *>(smraw);          // ternary psi ring
+  float2 *ringP2 = reinterpret_cast<float2 *>(smraw);          // binary psi ring
+  float4 *ringB = reinterpret_cast<float4 *>(smraw + G::P_BYTES);
+  float *stage = reinterpret_cast<float *>(smraw + G::P_BYTES + G::B_BYTES);
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  float *mystage = stage + tid;
+
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    const LatDesc &Lg = lats[T.lat];
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    const int base = (int)Lg.base;
+    const int par = Lg.parity;
+    const float *__restrict__ F = (par ? f1 : f0) + base;
+    float *__restrict__ Fo = (par ? f0 : f1) + base;
+    const float *__restrict__ DBn = (NC == 3) ? (par ? db0 : db1) + base : nullptr;  // new dipoles
+    const float4 *__restrict__ Mb = Mf + base;
+    const uint8_t *__restrict__ RK = rock + base;
+    const float rho0 = Lg.rho0, psi0 = Lg.psi0;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const bool small = (nx < TX + 2) || (ny < TY + 2);
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool act = gx < nx && gy < ny;
+
+    // ring index r holds plane z0 - 1 + r in slot r % RS
+    auto load_ring = [&](int r) {
+      const int gz = pmod(z0 - 1 + r, nz);
+      const int sl = (r % RS) * AN;
+      for (int s = tid; s < AN; s += NT) {
+        const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
+        const int ix = small ? pmod(vx, nx) : wrap_small(vx, nx);
+        const int iy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        const int i = ix + nx * (iy + ny * gz);
+        if (NC == 3) {
+          cp_async16(ringP4 + sl + s, Mb + S + i);  // {da_z, dpsi_r, dpsi_b, dpsi_s}
+          float *b = reinterpret_cast<float *>(ringB + sl + s);
+          cp_async4(b, DBn + i);
+          cp_async4(b + 1, DBn + S + i);
+          cp_async4(b + 2, DBn + 2 * S + i);
+        } else {
+          cp_async8(ringP2 + sl + s, reinterpret_cast<const float2 *>(Mb) + i);
+        }
+      }
+    };
+    // own-site pulls of compute plane k into the stage; returns the own rock flag
+    auto issue_pulls = [&](int k) -> bool {
+      if (!act) return true;
+      Nbr nb;
+      make_nbr(nb, gx, gy, pmod(z0 + k, nz), nx, ny, nz);
+      const int self = noff<18, 1>(nb);
+      if (ROCK && __ldg(RK + self) != 0) return true;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) pull_async<ROCK, NT>(F, S, c, nb, self, RK, mystage + c * 19 * NT);
+      return false;
+    };
+
+    load_ring(0);
+    load_ring(1);
+    load_ring(2);
+    cp_async_commit();
+    bool skip = issue_pulls(0);
+    cp_async_commit();
+
+    for (int k = 0; k < zc; ++k) {
+      if (k + 3 <= zc + 1) load_ring(k + 3);
+      cp_async_commit();
+      cp_async_wait<2>();  // ring planes up to k + 2 landed (this thread's copies)
+      __syncthreads();     // ... and everybody's
+      const int gzc = pmod(z0 + k, nz);
+      float Fx[NC][3];
+      Nbr nb;
+      int self = 0;
+      if (act && !skip) {
+        make_nbr(nb, gx, gy, gzc, nx, ny, nz);
+        self = noff<18, 1>(nb);
+        const int as = (tx + 1) + AW * (ty + 1);
+        if constexpr (NC == 3) {
+          force_ternary<AW>(ringP4 + (k % RS) * AN, ringP4 + ((k + 1) % RS) * AN,
+                            ringP4 + ((k + 2) % RS) * AN, ringB + (k % RS) * AN,
+                            ringB + ((k + 1) % RS) * AN, ringB + ((k + 2) % RS) * AN, as, Lg, psi0,
+                            reinterpret_cast<float(*)[3]>(Fx));
+        } else {
+          // binary rings hold {dpsi_r, dpsi_b}
+          const float2 *Qm = ringP2 + (k % RS) * AN, *Q0 = ringP2 + ((k + 1) % RS) * AN,
+                       *Qp = ringP2 + ((k + 2) % RS) * AN;
+          force_binary<AW, ROCK>(Qm, Q0, Qp, as, nb, RK, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
+        }
+      }
+      cp_async_wait<1>();  // this thread's pulls of plane k landed
+      if (act && !skip) {
+        float dr[NC], rho[NC], j[NC][3];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float *sc = mystage + c * 19 * NT;
+          float acc = 0.0f;
+#pragma unroll
+          for (int q = 0; q < 19; ++q) acc = fmaf((float)gw(q), sc[q * NT], acc);
+          dr[c] = acc;
+          rho[c] = rho0 + acc;
+          float j0 = 0.f, j1 = 0.f, j2 = 0.f;
+#pragma unroll
+          for (int q = 0; q < 19; ++q) {
+            const float ng = (float)gw(q) * sc[q * NT];
+            if (cx(q)) j0 += cx(q) * ng;
+            if (cy(q)) j1 += cy(q) * ng;
+            if (cz(q)) j2 += cz(q) * ng;
+          }
+          j[c][0] = j0;
+          j[c][1] = j1;
+          j[c][2] = j2;
+        }
+        if (BODY) {
+          const int x1 = gx + 1, y1 = gy + 1, z1 = gzc + 1;
+          bool on;
+          if (Lg.inv_fluid == 9)
+            on = (z1 == 1) || (z1 == nz);
+          else if (Lg.inv_fluid == 20 || Lg.inv_fluid == 21)
+            on = z1 == 1;
+          else
+            on = z1 >= Lg.amin_z && z1 <= Lg.amax_z && x1 >= Lg.amin_x && x1 <= Lg.amax_x &&
+                 y1 >= Lg.amin_y && y1 <= Lg.amax_y;
+          if (on) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const float m = Lg.amass[c] * rho[c];
+              Fx[c][0] = fmaf(m, Lg.g_accn_x, Fx[c][0]);
+              Fx[c][1] = fmaf(m, Lg.g_accn_y, Fx[c][1]);
+              Fx[c][2] = fmaf(m, Lg.g_accn, Fx[c][2]);
+            }
+          }
+        }
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f, rt = 0.f;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float am = Lg.amass[c] * Lg.omega[c];
+          p0 = fmaf(am, j[c][0], p0);
+          p1 = fmaf(am, j[c][1], p1);
+          p2 = fmaf(am, j[c][2], p2);
+          rt = fmaf(am, rho[c], rt);
+        }
+        const float irt = 1.0f / fmaxf(rt, 1.0e-8f);
+        const float u0 = p0 * irt, u1 = p1 * irt, u2 = p2 * irt;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float kf = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
+          float d[19];
+          const float *sc = mystage + c * 19 * NT;
+#pragma unroll
+          for (int q = 0; q < 19; ++q) d[q] = sc[q * NT];
+          bgk_update(d, rho[c], dr[c], fmaf(kf, Fx[c][0], u0), fmaf(kf, Fx[c][1], u1),
+                     fmaf(kf, Fx[c][2], u2), Lg.omega[c]);
+          float *fo = Fo + c * 19 * S + self;
+#pragma unroll
+          for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
+        }
+      }
+      // the stage column is free again: start the next plane's pulls
+      skip = (k + 1 < zc) ? issue_pulls(k + 1) : true;
+      cp_async_commit();
+    }
+    cp_async_wait<0>();
+    __syncthreads();  // the next tile refills ring slots 0..2
   }
 }

@@ -102,7 +102,7 @@ def _params(L, nc, **kw):
 
 
 def test_binary_64cube_1000_steps_parity():
-    """binary 64^3 periodic, g_br=0.08, 1000 steps; the
+    """Binary 64^3 periodic, g_br=0.08, 1000 steps; the
     plain path must match to 1e-12 relative per site (here: exactly)."""
     p = _params((64, 64, 64), 2)
     st = uniform_mixture(64, 64, 64, 2, seed=1)
