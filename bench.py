@@ -189,7 +189,7 @@ def serving(rank, size, nreq=96, seq_sample=4):
     from lb3d_b200.ic import uniform_mixture
     from lb3d_b200.lib import Lattice
     reqs = partition(sweep_requests(nreq, seed=7), rank, size)
-    ens = Ensemble(3, capacity_sites=24_000_000, max_lattices=2048, shape=(32, 4, 16, 1))
+    ens = Ensemble(3, capacity_sites=24_000_000, max_lattices=2048, shape=(16, 8, 8, 2))
     out = Server(ens, chunk=128, download=True).run(reqs)
     ens.close()
     seq = {}
@@ -296,6 +296,8 @@ def main():
     ap.add_argument("--configs", action="store_true", help="measure the four single-lattice workloads (binary 64^3 FP64, ternary 128^3 FP32 error, "
                     "Lees-Edwards 256x128x128, porous 256^3) instead")
     ap.add_argument("--error-steps", type=int, default=10000)
+    ap.add_argument("--shape", default=None,
+                    help="tx,ty,zc,split: fixed FP32 launch shape instead of the autotuner (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -319,7 +321,11 @@ def main():
     # ---- FP32 deviation path (headline) ----
     lat = Lattice(workload_params(precision=1))
     lat.upload_state(state)
-    shape, tune_ms = lat.autotune()
+    if args.shape:
+        lat.set_launch_shape(*[int(v) for v in args.shape.split(",")])
+        shape = lat.launch_shape
+    else:
+        shape, tune_ms = lat.autotune()
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -395,7 +401,9 @@ def main():
                        "lattice": [L, L, L], "g_br": 0.08, "g_bs": -0.006, "g_ss": -0.0045, "tau": 1.0,
                        "tau_d": 1.0, "beta": 10.0, "parallelism": f"replicas x{world}",
                        "l2": f"populations {2 * 57 * 4 * N / 1e6:.0f} MB > 126 MB L2, no flush",
-                       "launch_shape": list(shape[:3]), "strategy": "split" if shape[3] else "fused"},
+                       "launch_shape": list(shape[:3]),
+                       "strategy": ["fused", "split", "split, staged collide"][shape[3]],
+                       "shape_source": "fixed" if args.shape else "autotuned"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
                          "bytes_per_site": BYTES_PER_SITE[("f32", 3)], "kernel_ms_per_step": round(per_step_ms, 4)},

@@ -3,7 +3,9 @@
 nvcc cross-compiles for sm_100a without a GPU.  The FP64 drop-in kernels
 (fp64_path.cu) and the host-side C-ABI are compiled without FMA contraction
 (--fmad=false, -ffp-contract=off) so that they reproduce the CPU
-restatement bit for bit; the FP32 kernels keep contraction on.
+restatement bit for bit.  The FP32 kernels are compiled the same way and
+spell out each fused multiply-add they want (fmaf, paired __ffma2_rn), so
+every FP32 strategy rounds identically.
 """
 from __future__ import annotations
 
@@ -26,7 +28,9 @@ SOURCES = {
     "fp64_path.cu": ["--fmad=false"],
     "reduce.cu": ["--fmad=false"],
     "capi.cu": ["--fmad=false"],
-    "fp32_path.cu": [],
+    # the FP32 kernels spell out every fused multiply-add (fmaf, paired
+    # __ffma2_rn), so all strategies round identically
+    "fp32_path.cu": ["--fmad=false"],
     "ensemble.cu": [],
     "noalloc.cu": [],
 }

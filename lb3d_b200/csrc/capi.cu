@@ -110,6 +110,10 @@ int validate(const lb3dc_params *p, std::string &why) {
     return (why = "amass must be positive", LB3DC_EINVAL);
   if (p->precision != LB3DC_FP64 && p->precision != LB3DC_FP32_DEV)
     return (why = "precision must be LB3DC_FP64 or LB3DC_FP32_DEV", LB3DC_EINVAL);
+  if (p->precision == LB3DC_FP64 &&
+      (long long)p->nx * p->ny * p->nz + 2LL * p->ny * p->nz >= (1LL << 31))
+    return (why = "FP64 lattices are limited to 2^31 sites including the Lees-Edwards planes",
+            LB3DC_EINVAL);
   if (p->precision == LB3DC_FP32_DEV && le)
     return (why = "FP32 deviation storage is not implemented for Lees-Edwards", LB3DC_ENOTSUP);
   return LB3DC_OK;

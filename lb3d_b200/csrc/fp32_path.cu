@@ -52,7 +52,7 @@ __device__ __forceinline__ int pmod(int v, int n) {
 __device__ __forceinline__ float langevin(float x) {
   if (x < 0.3f) {
     float x2 = x * x;
-    return x * (1.0f / 3.0f + x2 * (-1.0f / 45.0f + x2 * (2.0f / 945.0f + x2 * (-1.0f / 4725.0f))));
+    return x * fmaf(x2, fmaf(x2, fmaf(x2, -1.0f / 4725.0f, 2.0f / 945.0f), -1.0f / 45.0f), 1.0f / 3.0f);
   }
   float t = tanhf(x);
   return 1.0f / t - 1.0f / x;
@@ -60,21 +60,22 @@ __device__ __forceinline__ float langevin(float x) {
 
 // Equilibrium deviation for one component: out_i = rho*(E_i(v) - w_i) + drho*w_i
 // with E of bdist = 2 (code/lb3d_bdist.F90:301-370), then the BGK update
-// d_i <- d_i + omega (deq_i - d_i).
+// d_i <- d_i + omega (deq_i - d_i).  Every multiply-add is written out
+// (fmaf), so bgk_update2 below can repeat the same roundings lane by lane.
 __device__ __forceinline__ void bgk_update(float d[19], float rho, float drho, float vx, float vy,
                                            float vz, float omega) {
   const float tx = 3.0f * vx, ty = 3.0f * vy, tz = 3.0f * vz;
-  const float uke = 0.5f * (tx * vx + ty * vy + tz * vz);
+  const float uke = 0.5f * fmaf(tz, vz, fmaf(ty, vy, tx * vx));
   const float a = -uke;          // even part minus w
-  const float b = 1.0f - uke;    // odd linear coefficient
+  const float b = 1.0f + a;      // odd linear coefficient
   const float rw = rho * W1;
   const float base = drho * W1;
 #define LB3D_PAIR32(CD, I, J)                                             \
   {                                                                       \
     const float e = (CD);                                                 \
     const float e2 = e * e;                                               \
-    const float ev = rw * fmaf(0.5f, e2, a) + base;                       \
-    const float od = rw * e * fmaf(e2, 1.0f / 6.0f, b);                   \
+    const float ev = fmaf(rw, fmaf(0.5f, e2, a), base);                   \
+    const float od = (rw * e) * fmaf(e2, 1.0f / 6.0f, b);                 \
     d[I] = fmaf(omega, (ev + od) - d[I], d[I]);                           \
     d[J] = fmaf(omega, (ev - od) - d[J], d[J]);                           \
   }
@@ -88,8 +89,89 @@ __device__ __forceinline__ void bgk_update(float d[19], float rho, float drho, f
   LB3D_PAIR32(ty + tz, 14, 17)
   LB3D_PAIR32(ty - tz, 15, 16)
 #undef LB3D_PAIR32
-  const float deq0 = rho * W0 * a + drho * W0;
+  const float deq0 = fmaf(rho * W0, a, drho * W0);
   d[18] = fmaf(omega, deq0 - d[18], d[18]);
+}
+
+// Paired FP32 arithmetic (sm_100 FADD2/FMUL2/FFMA2: two lanes per
+// instruction, each rounded as its scalar counterpart).
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// bgk_update for two components at once (lane x, lane y), bit for bit the
+// scalar routine on each lane.
+__device__ __forceinline__ void bgk_update2(float2 d[19], float2 rho, float2 drho, float2 vx,
+                                            float2 vy, float2 vz, float2 omega) {
+  const float2 tx = mul2(f2(3.0f), vx), ty = mul2(f2(3.0f), vy), tz = mul2(f2(3.0f), vz);
+  const float2 uke = mul2(f2(0.5f), fma2(tz, vz, fma2(ty, vy, mul2(tx, vx))));
+  const float2 a = neg2(uke);
+  const float2 b = add2(f2(1.0f), a);
+  const float2 rw = mul2(rho, f2(W1));
+  const float2 base = mul2(drho, f2(W1));
+#define LB3D_PAIR2(CD, I, J)                                                  \
+  {                                                                           \
+    const float2 e = (CD);                                                    \
+    const float2 e2 = mul2(e, e);                                             \
+    const float2 ev = fma2(rw, fma2(f2(0.5f), e2, a), base);                  \
+    const float2 od = mul2(mul2(rw, e), fma2(e2, f2(1.0f / 6.0f), b));        \
+    d[I] = fma2(omega, add2(add2(ev, od), neg2(d[I])), d[I]);                 \
+    d[J] = fma2(omega, add2(add2(ev, neg2(od)), neg2(d[J])), d[J]);           \
+  }
+  LB3D_PAIR2(tx, 0, 1)
+  LB3D_PAIR2(ty, 2, 3)
+  LB3D_PAIR2(tz, 4, 5)
+  LB3D_PAIR2(add2(tx, ty), 6, 11)
+  LB3D_PAIR2(add2(tx, neg2(ty)), 7, 10)
+  LB3D_PAIR2(add2(tx, tz), 8, 13)
+  LB3D_PAIR2(add2(tx, neg2(tz)), 9, 12)
+  LB3D_PAIR2(add2(ty, tz), 14, 17)
+  LB3D_PAIR2(add2(ty, neg2(tz)), 15, 16)
+#undef LB3D_PAIR2
+  const float2 deq0 = fma2(mul2(rho, f2(W0)), a, mul2(drho, f2(W0)));
+  d[18] = fma2(omega, add2(deq0, neg2(d[18])), d[18]);
+}
+
+// Own-site moments of one component's post-stream deviations d[q * ST]:
+// drho = sum_q g_q d_q and j = sum_q g_q c_q d_q, in q order, one fused
+// multiply-add per term.
+template <int ST>
+__device__ __forceinline__ void own_moments(const float *d, float &dr, float &j0, float &j1,
+                                            float &j2) {
+  float r = 0.f, a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const float v = d[q * ST], g = (float)gw(q);
+    r = fmaf(g, v, r);
+    if (cx(q)) a0 = fmaf(g * (float)cx(q), v, a0);
+    if (cy(q)) a1 = fmaf(g * (float)cy(q), v, a1);
+    if (cz(q)) a2 = fmaf(g * (float)cz(q), v, a2);
+  }
+  dr = r;
+  j0 = a0;
+  j1 = a1;
+  j2 = a2;
+}
+// own_moments of two components (lanes x, y) with paired instructions.
+template <int ST>
+__device__ __forceinline__ void own_moments2(const float *dA, const float *dB, float2 &dr,
+                                             float2 &j0, float2 &j1, float2 &j2) {
+  float2 r = f2(0.f), a0 = f2(0.f), a1 = f2(0.f), a2 = f2(0.f);
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const float2 v = make_float2(dA[q * ST], dB[q * ST]);
+    const float g = (float)gw(q);
+    r = fma2(f2(g), v, r);
+    if (cx(q)) a0 = fma2(f2(g * (float)cx(q)), v, a0);
+    if (cy(q)) a1 = fma2(f2(g * (float)cy(q)), v, a1);
+    if (cz(q)) a2 = fma2(f2(g * (float)cz(q)), v, a2);
+  }
+  dr = r;
+  j0 = a0;
+  j1 = a1;
+  j2 = a2;
 }
 
 // Site offsets (32-bit, relative to the lattice base) of the -1, 0, +1
@@ -158,6 +240,8 @@ __device__ __forceinline__ int wrap_small(int v, int n) {
   // valid for -n <= v < 2n
   return v < 0 ? v + n : (v >= n ? v - n : v);
 }
+
+#include "fp32_stencil.cuh"
 
 // Kernel modes.  FUSED: one pass per step (moments recomputed on the halo).
 // MOMENTS + COLLIDE: the split strategy, two passes per step: MOMENTS
@@ -258,22 +342,13 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           for (int c = 0; c < NC; ++c) {
             float d[19];
             pull_comp<ROCK>(F, S, c, nb, self, RK, d);
-            float acc = 0.0f;
-#pragma unroll
-            for (int q = 0; q < 19; ++q) acc = fmaf((float)gw(q), d[q], acc);
-            dr[c] = acc;
             if (MODE == MODE_MOMENTS) {
-              float j0 = 0.f, j1 = 0.f, j2 = 0.f;
+              own_moments<1>(d, dr[c], jm[c][0], jm[c][1], jm[c][2]);
+            } else {
+              float acc = 0.0f;
 #pragma unroll
-              for (int q = 0; q < 19; ++q) {
-                const float ng = (float)gw(q) * d[q];
-                if (cx(q)) j0 += cx(q) * ng;
-                if (cy(q)) j1 += cy(q) * ng;
-                if (cz(q)) j2 += cz(q) * ng;
-              }
-              jm[c][0] = j0;
-              jm[c][1] = j1;
-              jm[c][2] = j2;
+              for (int q = 0; q < 19; ++q) acc = fmaf((float)gw(q), d[q], acc);
+              dr[c] = acc;
             }
             if (NC == 3 && c == 2) {
               // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
@@ -283,7 +358,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
               for (int q = 0; q < 19; ++q) {
                 const float4 *Dq = cz(q) == 1 ? Dm : (cz(q) == -1 ? Dp : D0);
                 const float4 b = Dq[ds0 - cx(q) - DW * cy(q)];
-                const float ng = (float)gw(q) * (d[q] + wq(q) * rho0);
+                const float ng = (float)gw(q) * fmaf(wq(q), rho0, d[q]);
                 a0 = fmaf(ng, b.x, a0);
                 a1 = fmaf(ng, b.y, a1);
                 a2 = fmaf(ng, b.z, a2);
@@ -326,47 +401,17 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
       __syncthreads();
       if (MODE == MODE_MOMENTS) continue;
       // ---------------- stage B (ternary): dipole relaxation ----------------
-      if (NC == 3 && it >= 2) {
+      if constexpr (NC == 3) if (it >= 2) {
         float4 *slotB = ringB + (it % 3) * BN;
         const int zB = zA - 1;
-        const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
         const float4 *Am = ringA + ((it - 2) % AR) * AV * AN;  // plane zB - 1
         const float4 *A0 = ringA + ((it - 1) % AR) * AV * AN;  // plane zB
         const float4 *Ap = ringA + ((it) % AR) * AV * AN;      // plane zB + 1
         for (int s = tid; s < BN; s += NT) {
           const int bx = s % BW, by = s / BW;
           const int as = (bx + 1) + AW * (by + 1);
-          const float4 own0 = A0[as];  // {rho_b - rho_r, da}
-          const float own_drs = A0[AN + as].x;
-          float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
-          float hs0 = own0.y, hs1 = own0.z, hs2 = own0.w;
-          const float isN = 1.0f / fmaxf(rho0 + own_drs, 1.0e-4f);
-#pragma unroll
-          for (int q = 0; q < 18; ++q) {
-            const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-            const int an = as + cx(q) + AW * cy(q);
-            const float4 e0 = Aq[an];
-            const float g = (float)gw(q);
-            const float hcm = -sgn * e0.x * g;  // e0.x = rho_b - rho_r
-            const float dot2 = 2.0f * (cx(q) * e0.y + cy(q) * e0.z + cz(q) * e0.w);
-            if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
-            if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
-            if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
-            hs0 = fmaf(e0.y - cx(q) * dot2, g, hs0);
-            hs1 = fmaf(e0.z - cy(q) * dot2, g, hs1);
-            hs2 = fmaf(e0.w - cz(q) * dot2, g, hs2);
-          }
-          const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
-          const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
-          const float hm = Lg.beta * hn;
-          // d_eq = d0 L(beta|h|) h/|h| with the Langevin function L; the
-          // reference's small-field branch beta h / 3 (h_m <= 0.01) is L's
-          // first-order term.
-          const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
-          const float od = Lg.omega_d, om1 = (1.0f - od) * isN;
-          const float n0 = od * fac * h0 + om1 * own0.y;
-          const float n1 = od * fac * h1 + om1 * own0.z;
-          const float n2 = od * fac * h2 + om1 * own0.w;
+          const float3 nd = dipole_site<AW>(Am, A0, Ap, as, Lg, rho0, A0[AN + as].x);
+          const float n0 = nd.x, n1 = nd.y, n2 = nd.z;
           slotB[s] = make_float4(n0, n1, n2, 0.0f);
           if (bx >= 1 && bx <= TX && by >= 1 && by <= TY && zB >= z0 && zB < z0 + zc) {
             const int gx = x0 + bx - 1, gy = y0 + by - 1;
@@ -398,125 +443,17 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
             const float4 *A0 = ringA + (itC % AR) * AV * AN;
             const float4 *Ap = ringA + ((itC + 1) % AR) * AV * AN;
             float Fx[NC][3];
-            float psi_own[NC];
-            if (NC == 3) {
-              // ---- ternary Shan-Chen force, code/lb3d_force_shanchen.F90:215-330,
-              // accumulated as moments of the neighbour terms so that the own
-              // dipole d enters once at the end:
-              //   f_cs = SA - 2 V,            SA = sum g a,  V = sum g (a.c) c
-              //   f_sc = SG d - 2 T d,        SG = sum G, T = sum G c c^T, G = g (psi_b - psi_r)
-              //   f_ss = M^T d + M d + tr(M) d - 2 Q d,
-              //                               M = sum 8g a c^T, Q = sum 8g (a.c) c c^T
-              // with a = d(y) psi_s(y) the neighbour's dipole times its psi.
+            if constexpr (NC == 3) {
+              // ---- ternary Shan-Chen force, code/lb3d_force_shanchen.F90:215-330
               const int itB = itC + 1;  // B computed plane zC at iteration itC + 1
               const int bs = (tx + 1) + BW * (ty + 1);
-              const float4 *Bm = ringB + ((itB + 2) % 3) * BN;
-              const float4 *B0 = ringB + (itB % 3) * BN;
-              const float4 *Bp = ringB + ((itB + 1) % 3) * BN;
-              float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, SA[3] = {0, 0, 0}, V[3] = {0, 0, 0};
-              float SG = 0.f, T[6] = {0, 0, 0, 0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0};
-              float M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-              for (int q = 0; q < 18; ++q) {
-                const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-                const float4 *Bq = cz(q) == 1 ? Bp : (cz(q) == -1 ? Bm : B0);
-                const int an = as + cx(q) + AW * cy(q);
-                const int bn = bs + cx(q) + BW * cy(q);
-                const float g = (float)gw(q);
-                const int c[3] = {cx(q), cy(q), cz(q)};
-                const float4 e = Aq[AN + an];  // {drho_s, dpsi_r, dpsi_b, dpsi_s}
-                const float4 b = Bq[bn];
-                const float ps = psi0 + e.w;
-                const float a[3] = {b.x * ps, b.y * ps, b.z * ps};
-                float ac = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                  if (c[k]) ac = fmaf((float)c[k], a[k], ac);
-                const float Gq = g * (e.z - e.y);
-                const float g8 = 8.0f * g;
-                SG += Gq;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                  SA[k] = fmaf(g, a[k], SA[k]);
-                  if (c[k]) {
-                    frb[k] = fmaf(g * (float)c[k], e.z, frb[k]);
-                    fbr[k] = fmaf(g * (float)c[k], e.y, fbr[k]);
-                    V[k] = fmaf(g * (float)c[k], ac, V[k]);
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) M[i][k] = fmaf(g8 * (float)c[k], a[i], M[i][k]);
-                  }
-                }
-                // symmetric c c^T: entries xx yy zz xy xz yz
-#define LB3D_SYM(I, J, K)                                      \
-  if (c[I] && c[J]) {                                          \
-    const float cc = (float)(c[I] * c[J]);                     \
-    T[K] = fmaf(Gq, cc, T[K]);                                 \
-    Q[K] = fmaf(g8 * ac, cc, Q[K]);                            \
-  }
-                LB3D_SYM(0, 0, 0) LB3D_SYM(1, 1, 1) LB3D_SYM(2, 2, 2)
-                LB3D_SYM(0, 1, 3) LB3D_SYM(0, 2, 4) LB3D_SYM(1, 2, 5)
-#undef LB3D_SYM
-              }
-              const float4 dd = B0[bs];
-              const float d[3] = {dd.x, dd.y, dd.z};
-              const float4 own = A0[AN + as];
-              psi_own[0] = psi0 + own.y;
-              psi_own[1] = psi0 + own.z;
-              psi_own[NC - 1] = psi0 + own.w;
-              const float Td[3] = {T[0] * d[0] + T[3] * d[1] + T[4] * d[2],
-                                   T[3] * d[0] + T[1] * d[1] + T[5] * d[2],
-                                   T[4] * d[0] + T[5] * d[1] + T[2] * d[2]};
-              const float Qd[3] = {Q[0] * d[0] + Q[3] * d[1] + Q[4] * d[2],
-                                   Q[3] * d[0] + Q[1] * d[1] + Q[5] * d[2],
-                                   Q[4] * d[0] + Q[5] * d[1] + Q[2] * d[2]};
-              const float trM = M[0][0] + M[1][1] + M[2][2];
-#pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                const float MTd = M[0][k] * d[0] + M[1][k] * d[1] + M[2][k] * d[2];
-                const float Md = M[k][0] * d[0] + M[k][1] * d[1] + M[k][2] * d[2];
-                const float fcs = SA[k] - 2.0f * V[k];
-                const float fsc = SG * d[k] - 2.0f * Td[k];
-                const float fss = MTd + Md + trM * d[k] - 2.0f * Qd[k];
-                const float cs = -2.0f * Lg.g_bs * fcs;
-                Fx[1][k] = (-Lg.g_br * fbr[k] + cs) * psi_own[1];
-                Fx[0][k] = (-Lg.g_br * frb[k] - cs) * psi_own[0];
-                Fx[NC - 1][k] = (2.0f * Lg.g_bs * fsc - Lg.g_ss * fss) * psi_own[NC - 1];
-              }
+              force_ternary<AW, BW>(Am + AN, A0 + AN, Ap + AN, ringB + ((itB + 2) % 3) * BN,
+                                    ringB + (itB % 3) * BN, ringB + ((itB + 1) % 3) * BN, as, bs, Lg,
+                                    psi0, reinterpret_cast<float(*)[3]>(Fx));
             } else {
               // ---- binary Shan-Chen force with walls, :127-210
-              float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
-#pragma unroll
-              for (int q = 0; q < 18; ++q) {
-                const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-                const int an = as + cx(q) + AW * cy(q);
-                const float g = (float)gw(q);
-                const int c[3] = {cx(q), cy(q), cz(q)};
-                bool nrock = false;
-                if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
-                // a rock neighbour contributes psi(0 + rock colour) to the
-                // wall sums; the fluid sums run over fluid neighbours only,
-                // so their psi(rho0) share no longer cancels and is removed.
-                const float4 e = Aq[an];
-                const float pr = nrock ? -psi0 : e.x, pb = nrock ? -psi0 : e.y;
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                  if (c[k]) {
-                    frb[k] = fmaf(pb * g, (float)c[k], frb[k]);
-                    fbr[k] = fmaf(pr * g, (float)c[k], fbr[k]);
-                    if (ROCK && nrock) {
-                      fwb[k] = fmaf(Lg.psiw_b * g, (float)c[k], fwb[k]);
-                      fwr[k] = fmaf(Lg.psiw_r * g, (float)c[k], fwr[k]);
-                    }
-                  }
-              }
-              const float4 own = A0[as];
-              psi_own[0] = psi0 + own.x;
-              psi_own[1] = psi0 + own.y;
-#pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                Fx[1][k] = (-Lg.g_br * fbr[k] + Lg.wall_b * fwb[k]) * psi_own[1];
-                Fx[0][k] = (-Lg.g_br * frb[k] + Lg.wall_r * fwr[k]) * psi_own[0];
-              }
+              force_binary<AW, ROCK>(Am, A0, Ap, as, nb, RK, Lg, psi0,
+                                     reinterpret_cast<float(*)[3]>(Fx));
             }
             // ---- pass 1: moments of the own post-stream populations (the
             // pulls hit L2: stage A fetched them H planes earlier)
@@ -525,19 +462,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
             for (int c = 0; c < NC; ++c) {
               float d[19];
               pull_comp<ROCK>(F, S, c, nb, self, RK, d);
-              float r = 0.f, j0 = 0.f, j1 = 0.f, j2 = 0.f;
-#pragma unroll
-              for (int q = 0; q < 19; ++q) {
-                const float ng = (float)gw(q) * d[q];
-                r += ng;
-                if (cx(q)) j0 += cx(q) * ng;
-                if (cy(q)) j1 += cy(q) * ng;
-                if (cz(q)) j2 += cz(q) * ng;
-              }
-              dr[c] = r;
-              j[c][0] = j0;
-              j[c][1] = j1;
-              j[c][2] = j2;
+              own_moments<1>(d, dr[c], j[c][0], j[c][1], j[c][2]);
             }
             float rho[NC];
 #pragma unroll
@@ -881,10 +806,11 @@ long long fp32_footprint(const lb3dc_params &p) {
          N * (fp32_moment_bytes(p.ncomp) + fp32_own_bytes(p.ncomp)) + 4096;
 }
 
+// Shape before any autotuning: the split strategy with the staged collide
+// pass, which measured fastest on 128^3 ternary and 256^3 binary lattices.
 static FusedShape default_shape(const DevParams &P) {
-  FusedShape sh{32, 8, 16, P.nc == 3 ? 1 : 0};
-  if (P.nx < 32) sh = FusedShape{16, 16, 16};
-  if (P.nc == 2) sh.zc = 32;
+  FusedShape sh{32, 4, P.nc == 3 ? 8 : 16, 2};
+  if (P.nx < 32) sh.tx = 16, sh.ty = 8;
   return sh;
 }
 

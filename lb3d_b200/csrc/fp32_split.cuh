@@ -16,152 +16,6 @@
 // memory while marching in z, so every field is loaded from global memory
 // once per tile plane (halos hit L2).
 
-// Dipole relaxation of one site (code/lb3d_collision.F90:296-403) from the
-// ring planes of moment entries {rho_b - rho_r, da_x, da_y, da_z} (row
-// stride AW) and the site's own surfactant density deviation.
-template <int AW>
-__device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0, const float4 *Ap,
-                                              int as, const LatDesc &Lg, float rho0, float own_drs) {
-  const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
-  const float4 own0 = A0[as];
-  float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
-  float hs0 = own0.y, hs1 = own0.z, hs2 = own0.w;
-  const float isN = 1.0f / fmaxf(rho0 + own_drs, 1.0e-4f);
-#pragma unroll
-  for (int q = 0; q < 18; ++q) {
-    const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-    const float4 e0 = Aq[as + cx(q) + AW * cy(q)];
-    const float g = (float)gw(q);
-    const float hcm = -sgn * e0.x * g;
-    const float dot2 = 2.0f * (cx(q) * e0.y + cy(q) * e0.z + cz(q) * e0.w);
-    if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
-    if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
-    if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
-    hs0 = fmaf(e0.y - cx(q) * dot2, g, hs0);
-    hs1 = fmaf(e0.z - cy(q) * dot2, g, hs1);
-    hs2 = fmaf(e0.w - cz(q) * dot2, g, hs2);
-  }
-  const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
-  const float hn = sqrtf(h0 * h0 + h1 * h1 + h2 * h2);
-  const float hm = Lg.beta * hn;
-  const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
-  const float od = Lg.omega_d, om1 = (1.0f - od) * isN;
-  return make_float3(od * fac * h0 + om1 * own0.y, od * fac * h1 + om1 * own0.z,
-                     od * fac * h2 + om1 * own0.w);
-}
-
-// Ternary Shan-Chen force (code/lb3d_force_shanchen.F90:215-330) of one
-// site from psi entries P = {-, dpsi_r, dpsi_b, dpsi_s} and dipole entries B
-// (stride W in both), accumulated as neighbour moments so that the own
-// dipole d enters once:
-//   f_cs = SA - 2V, f_sc = SG d - 2 T d, f_ss = M^T d + M d + tr(M) d - 2 Q d
-// with a = d(y) psi_s(y), SA = sum g a, V = sum g (a.c) c, G = g (psi_b -
-// psi_r), SG = sum G, T = sum G c c^T, M = sum 8g a c^T, Q = sum 8g (a.c) c c^T.
-template <int W>
-__device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0, const float4 *Pp,
-                                              const float4 *Bm, const float4 *B0, const float4 *Bp,
-                                              int as, const LatDesc &Lg, float psi0, float Fx[3][3]) {
-  float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, SA[3] = {0, 0, 0}, V[3] = {0, 0, 0};
-  float SG = 0.f, T[6] = {0, 0, 0, 0, 0, 0}, Q[6] = {0, 0, 0, 0, 0, 0};
-  float M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-  for (int q = 0; q < 18; ++q) {
-    const float4 *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
-    const float4 *Bq = cz(q) == 1 ? Bp : (cz(q) == -1 ? Bm : B0);
-    const int an = as + cx(q) + W * cy(q);
-    const float g = (float)gw(q);
-    const int c[3] = {cx(q), cy(q), cz(q)};
-    const float4 e = Pq[an];
-    const float4 b = Bq[an];
-    const float ps = psi0 + e.w;
-    const float a[3] = {b.x * ps, b.y * ps, b.z * ps};
-    float ac = 0.f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      if (c[k]) ac = fmaf((float)c[k], a[k], ac);
-    const float Gq = g * (e.z - e.y);
-    const float g8 = 8.0f * g;
-    SG += Gq;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      SA[k] = fmaf(g, a[k], SA[k]);
-      if (c[k]) {
-        frb[k] = fmaf(g * (float)c[k], e.z, frb[k]);
-        fbr[k] = fmaf(g * (float)c[k], e.y, fbr[k]);
-        V[k] = fmaf(g * (float)c[k], ac, V[k]);
-#pragma unroll
-        for (int i = 0; i < 3; ++i) M[i][k] = fmaf(g8 * (float)c[k], a[i], M[i][k]);
-      }
-    }
-#define LB3D_SYM(I, J, K)                  \
-  if (c[I] && c[J]) {                      \
-    const float cc = (float)(c[I] * c[J]); \
-    T[K] = fmaf(Gq, cc, T[K]);             \
-    Q[K] = fmaf(g8 * ac, cc, Q[K]);        \
-  }
-    LB3D_SYM(0, 0, 0) LB3D_SYM(1, 1, 1) LB3D_SYM(2, 2, 2)
-    LB3D_SYM(0, 1, 3) LB3D_SYM(0, 2, 4) LB3D_SYM(1, 2, 5)
-#undef LB3D_SYM
-  }
-  const float4 dd = B0[as];
-  const float d[3] = {dd.x, dd.y, dd.z};
-  const float4 own = P0[as];
-  const float psr = psi0 + own.y, psb = psi0 + own.z, pss = psi0 + own.w;
-  const float Td[3] = {T[0] * d[0] + T[3] * d[1] + T[4] * d[2], T[3] * d[0] + T[1] * d[1] + T[5] * d[2],
-                       T[4] * d[0] + T[5] * d[1] + T[2] * d[2]};
-  const float Qd[3] = {Q[0] * d[0] + Q[3] * d[1] + Q[4] * d[2], Q[3] * d[0] + Q[1] * d[1] + Q[5] * d[2],
-                       Q[4] * d[0] + Q[5] * d[1] + Q[2] * d[2]};
-  const float trM = M[0][0] + M[1][1] + M[2][2];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float MTd = M[0][k] * d[0] + M[1][k] * d[1] + M[2][k] * d[2];
-    const float Md = M[k][0] * d[0] + M[k][1] * d[1] + M[k][2] * d[2];
-    const float fcs = SA[k] - 2.0f * V[k];
-    const float fsc = SG * d[k] - 2.0f * Td[k];
-    const float fss = MTd + Md + trM * d[k] - 2.0f * Qd[k];
-    const float cs = -2.0f * Lg.g_bs * fcs;
-    Fx[1][k] = (-Lg.g_br * fbr[k] + cs) * psb;
-    Fx[0][k] = (-Lg.g_br * frb[k] - cs) * psr;
-    Fx[2][k] = (2.0f * Lg.g_bs * fsc - Lg.g_ss * fss) * pss;
-  }
-}
-
-// Binary force with walls (:127-210) from psi entries {dpsi_r, dpsi_b, -, -}.
-template <int W, bool ROCK, typename E>
-__device__ __forceinline__ void force_binary(const E *Pm, const E *P0, const E *Pp,
-                                             int as, const Nbr &nb, const uint8_t *__restrict__ RK,
-                                             const LatDesc &Lg, float psi0, float Fx[2][3]) {
-  float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
-#pragma unroll
-  for (int q = 0; q < 18; ++q) {
-    const E *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
-    const int an = as + cx(q) + W * cy(q);
-    const float g = (float)gw(q);
-    const int c[3] = {cx(q), cy(q), cz(q)};
-    bool nrock = false;
-    if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
-    const E e = Pq[an];
-    const float pr = nrock ? -psi0 : e.x, pb = nrock ? -psi0 : e.y;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      if (c[k]) {
-        frb[k] = fmaf(pb * g, (float)c[k], frb[k]);
-        fbr[k] = fmaf(pr * g, (float)c[k], fbr[k]);
-        if (ROCK && nrock) {
-          fwb[k] = fmaf(Lg.psiw_b * g, (float)c[k], fwb[k]);
-          fwr[k] = fmaf(Lg.psiw_r * g, (float)c[k], fwr[k]);
-        }
-      }
-  }
-  const E own = P0[as];
-  const float psr = psi0 + own.x, psb = psi0 + own.y;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    Fx[1][k] = (-Lg.g_br * fbr[k] + Lg.wall_b * fwb[k]) * psb;
-    Fx[0][k] = (-Lg.g_br * frb[k] + Lg.wall_r * fwr[k]) * psr;
-  }
-}
-
 // Asynchronous copies global -> shared (cp.async, 4/8/16 bytes) in commit
 // groups; a thread waits for its own groups, a barrier then publishes them.
 __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
@@ -303,8 +157,8 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
             const float4 *Pm = ringP + ((it - 2) % 3) * AN, *P0 = ringP + ((it - 1) % 3) * AN;
             float Fx[NC][3];
             if (NC == 3)
-              force_ternary<AW>(Pm, P0, slotP, ringB + ((it - 2) % 3) * AN, ringB + ((it - 1) % 3) * AN,
-                                slotB, as, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
+              force_ternary<AW, AW>(Pm, P0, slotP, ringB + ((it - 2) % 3) * AN, ringB + ((it - 1) % 3) * AN,
+                                slotB, as, as, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
             else
               force_binary<AW, ROCK>(Pm, P0, slotP, as, nb, RK, Lg, psi0,
                                      reinterpret_cast<float(*)[3]>(Fx));
@@ -511,9 +365,9 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
         self = noff<18, 1>(nb);
         const int as = (tx + 1) + AW * (ty + 1);
         if constexpr (NC == 3) {
-          force_ternary<AW>(ringP4 + (k % RS) * AN, ringP4 + ((k + 1) % RS) * AN,
+          force_ternary<AW, AW>(ringP4 + (k % RS) * AN, ringP4 + ((k + 1) % RS) * AN,
                             ringP4 + ((k + 2) % RS) * AN, ringB + (k % RS) * AN,
-                            ringB + ((k + 1) % RS) * AN, ringB + ((k + 2) % RS) * AN, as, Lg, psi0,
+                            ringB + ((k + 1) % RS) * AN, ringB + ((k + 2) % RS) * AN, as, as, Lg, psi0,
                             reinterpret_cast<float(*)[3]>(Fx));
         } else {
           // binary rings hold {dpsi_r, dpsi_b}
@@ -525,25 +379,18 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
       cp_async_wait<1>();  // this thread's pulls of plane k landed
       if (act && !skip) {
         float dr[NC], rho[NC], j[NC][3];
+        {
+          // components 0 and 1 on paired lanes, the surfactant alone
+          float2 r2, a0, a1, a2;
+          own_moments2<NT>(mystage, mystage + 19 * NT, r2, a0, a1, a2);
+          dr[0] = r2.x, dr[1] = r2.y;
+          j[0][0] = a0.x, j[1][0] = a0.y;
+          j[0][1] = a1.x, j[1][1] = a1.y;
+          j[0][2] = a2.x, j[1][2] = a2.y;
+          if (NC == 3)
+            own_moments<NT>(mystage + 2 * 19 * NT, dr[NC - 1], j[NC - 1][0], j[NC - 1][1], j[NC - 1][2]);
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const float *sc = mystage + c * 19 * NT;
-          float acc = 0.0f;
-#pragma unroll
-          for (int q = 0; q < 19; ++q) acc = fmaf((float)gw(q), sc[q * NT], acc);
-          dr[c] = acc;
-          rho[c] = rho0 + acc;
-          float j0 = 0.f, j1 = 0.f, j2 = 0.f;
-#pragma unroll
-          for (int q = 0; q < 19; ++q) {
-            const float ng = (float)gw(q) * sc[q * NT];
-            if (cx(q)) j0 += cx(q) * ng;
-            if (cy(q)) j1 += cy(q) * ng;
-            if (cz(q)) j2 += cz(q) * ng;
-          }
-          j[c][0] = j0;
-          j[c][1] = j1;
-          j[c][2] = j2;
+          for (int c = 0; c < NC; ++c) rho[c] = rho0 + dr[c];
         }
         if (BODY) {
           const int x1 = gx + 1, y1 = gy + 1, z1 = gzc + 1;
@@ -576,16 +423,35 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
         }
         const float irt = 1.0f / fmaxf(rt, 1.0e-8f);
         const float u0 = p0 * irt, u1 = p1 * irt, u2 = p2 * irt;
+        float vx[NC], vy[NC], vz[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float kf = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
+          vx[c] = fmaf(kf, Fx[c][0], u0);
+          vy[c] = fmaf(kf, Fx[c][1], u1);
+          vz[c] = fmaf(kf, Fx[c][2], u2);
+        }
+        {
+          float2 d[19];
+#pragma unroll
+          for (int q = 0; q < 19; ++q) d[q] = make_float2(mystage[q * NT], mystage[(19 + q) * NT]);
+          bgk_update2(d, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+                      make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
+                      make_float2(Lg.omega[0], Lg.omega[1]));
+          float *fo = Fo + self;
+#pragma unroll
+          for (int q = 0; q < 19; ++q) {
+            __stcs(fo + q * S, d[q].x);
+            __stcs(fo + (19 + q) * S, d[q].y);
+          }
+        }
+        if (NC == 3) {
           float d[19];
-          const float *sc = mystage + c * 19 * NT;
+          const float *sc = mystage + 2 * 19 * NT;
 #pragma unroll
           for (int q = 0; q < 19; ++q) d[q] = sc[q * NT];
-          bgk_update(d, rho[c], dr[c], fmaf(kf, Fx[c][0], u0), fmaf(kf, Fx[c][1], u1),
-                     fmaf(kf, Fx[c][2], u2), Lg.omega[c]);
-          float *fo = Fo + c * 19 * S + self;
+          bgk_update(d, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1], Lg.omega[NC - 1]);
+          float *fo = Fo + 2 * 19 * S + self;
 #pragma unroll
           for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
         }

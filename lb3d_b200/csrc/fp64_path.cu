@@ -213,7 +213,7 @@ __global__ void k_le_halo(DevParams P, LEStep S, const double *__restrict__ src,
 // code/lb3d_bc_bounce.F90:53-90, code/lb3d_analysis.F90:64-102).
 // ---------------------------------------------------------------------------
 template <int NC, bool LE>
-__global__ void __launch_bounds__(256) k_stream(DevParams P, const double *__restrict__ fin,
+__global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__restrict__ fin,
                                                 double *__restrict__ fout, double *__restrict__ rho,
                                                 double *__restrict__ psi, double *__restrict__ mom,
                                                 double *__restrict__ da,
@@ -230,20 +230,21 @@ __global__ void __launch_bounds__(256) k_stream(DevParams P, const double *__res
   const bool fluid = rock[i] == 0;
   const long long NP = (long long)ny * nz;
 
-  // upstream index of each moving direction: -1/-2 mark the LE halos
-  long long up[18];
+  // upstream site of each moving direction (32-bit: the FP64 path bounds a
+  // lattice at 2^31 sites); negative values mark the LE halo planes
+  int up[18];
   bool upf[18];
 #pragma unroll
   for (int q = 0; q < 18; ++q) {
     int xu = x - cx(q), yu = wrap(y - cy(q), ny), zu = wrap(z - cz(q), nz);
     if (LE && xu < 0) {
-      up[q] = -1 - (yu + (long long)ny * zu);  // bottom halo
+      up[q] = -1 - (yu + ny * zu);  // bottom halo
       upf[q] = true;
     } else if (LE && xu >= nx) {
-      up[q] = -1 - NP - (yu + (long long)ny * zu);  // top halo
+      up[q] = -1 - (int)NP - (yu + ny * zu);  // top halo
       upf[q] = true;
     } else {
-      up[q] = sidx(wrap(xu, nx), yu, zu, nx, ny);
+      up[q] = (int)sidx(wrap(xu, nx), yu, zu, nx, ny);
       upf[q] = rock[up[q]] == 0;
     }
   }
@@ -258,6 +259,8 @@ __global__ void __launch_bounds__(256) k_stream(DevParams P, const double *__res
   };
 
   double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  // one component at a time keeps 19 pulls live, not 19*NC
+#pragma unroll 1
   for (int c = 0; c < NC; ++c) {
     double n[19];
 #pragma unroll

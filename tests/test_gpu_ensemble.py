@@ -8,7 +8,7 @@ from lb3d_b200.config import Params
 from lb3d_b200.ic import uniform_mixture
 
 pytestmark = pytest.mark.gpu
-SHAPE = (16, 8, 16, 1)  # tile 16x8, 16 planes, split strategy
+SHAPE = (16, 8, 16, 2)  # tile 16x8, 16 planes, split strategy with the staged collide
 
 
 def _p(L, nc=3, **kw):
