@@ -114,8 +114,7 @@ int validate(const lb3dc_params *p, std::string &why) {
       (long long)p->nx * p->ny * p->nz + 2LL * p->ny * p->nz >= (1LL << 31))
     return (why = "FP64 lattices are limited to 2^31 sites including the Lees-Edwards planes",
             LB3DC_EINVAL);
-  if (p->precision == LB3DC_FP32_DEV && le)
-    return (why = "FP32 deviation storage is not implemented for Lees-Edwards", LB3DC_ENOTSUP);
+
   return LB3DC_OK;
 }
 
@@ -522,7 +521,9 @@ int lb3dc_collision(lb3dc_handle *h) {
   } else {
     if (!h->pending_advection)
       return fail(h, LB3DC_ESTATE, "collision without a preceding advection");
-    rc = fp32_step(h->P, h->s32, h->rock, h->stream);
+    LEStep S;
+    if (h->le) S = le_step(h);
+    rc = fp32_step(h->P, h->s32, h->rock, h->stream, h->le ? &S : nullptr);
     if (rc) return fail(h, LB3DC_ECUDA, "FP32 step failed: %s", cudaGetErrorString(cudaGetLastError()));
     h->pending_advection = false;
   }
@@ -533,7 +534,7 @@ int lb3dc_time_loop(lb3dc_handle *h, int nsteps) {
   int rc = need_loaded(h);
   if (rc) return rc;
   if (nsteps < 0) return fail(h, LB3DC_EINVAL, "nsteps < 0");
-  if (h->p.precision == LB3DC_FP32_DEV) {
+  if (h->p.precision == LB3DC_FP32_DEV && !h->le) {
     h->nt += nsteps;
     rc = fp32_run(h->P, h->s32, h->rock, nsteps, h->stream);
     if (rc) return fail(h, LB3DC_ECUDA, "FP32 run failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -600,7 +601,9 @@ int lb3dc_autotune(lb3dc_handle *h, double *ms_out, int *ntried) {
   int rc = need_loaded(h);
   if (rc) return rc;
   if (h->p.precision != LB3DC_FP32_DEV) return fail(h, LB3DC_ENOTSUP, "autotune applies to the FP32 path");
-  rc = fp32_autotune(h->P, h->s32, h->rock, ms_out, ntried, h->stream);
+  LEStep S;
+  if (h->le) S = le_step(h);  // tune on this step's offset (the state is restored)
+  rc = fp32_autotune(h->P, h->s32, h->rock, ms_out, ntried, h->stream, h->le ? &S : nullptr);
   return rc ? fail(h, rc, "autotune failed: %s", cudaGetErrorString(cudaGetLastError())) : LB3DC_OK;
 }
 

@@ -35,6 +35,7 @@
 #include "fp32_path.h"
 #include "reduce.h"
 #include "fp64_path.h"
+#include "le_common.cuh"
 
 namespace lb3d {
 namespace f32 {
@@ -224,6 +225,41 @@ __device__ __forceinline__ void pull_comp(const float *__restrict__ F, int S, in
 #undef LB3D_PULL
 }
 
+// Lees-Edwards pulls (binary, no rock; code/lb3d_bc_leesedwards.F90:147-1315
+// feeding code/lb3d_advection.F90:109-151): across x = 0 (c_x = +1) and
+// x = nx - 1 (c_x = -1) the upstream site lies in the sheared halo planes
+// Lg.le_h[0] / Lg.le_h[1], [nc][19][nz][ny], at the wrapped (y - c_y, z - c_z).
+struct LeYZ {
+  int y[3], z[3];  // wrap(gy + k - 1) and ny * wrap(gz + k - 1)
+};
+__device__ __forceinline__ void make_leyz(LeYZ &w, int gy, int gz, int ny, int nz) {
+  w.y[0] = gy == 0 ? ny - 1 : gy - 1;
+  w.y[1] = gy;
+  w.y[2] = gy == ny - 1 ? 0 : gy + 1;
+  w.z[0] = ny * (gz == 0 ? nz - 1 : gz - 1);
+  w.z[1] = ny * gz;
+  w.z[2] = ny * (gz == nz - 1 ? 0 : gz + 1);
+}
+template <int Q>
+__device__ __forceinline__ const float *le_src(const float *fc, int S, int c, const Nbr &n, int gx,
+                                               int nx, const LeYZ &w, const LatDesc &Lg, int NP) {
+  if (cx(Q) == 1 && gx == 0) return Lg.le_h[0] + (c * 19 + Q) * NP + w.y[1 - cy(Q)] + w.z[1 - cz(Q)];
+  if (cx(Q) == -1 && gx == nx - 1)
+    return Lg.le_h[1] + (c * 19 + Q) * NP + w.y[1 - cy(Q)] + w.z[1 - cz(Q)];
+  return fc + Q * S + noff<Q, -1>(n);
+}
+__device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, int S, int c, const Nbr &n,
+                                             int self, int gx, int nx, const LeYZ &w,
+                                             const LatDesc &Lg, int NP, float d[19]) {
+  const float *fc = F + c * 19 * S;
+  d[18] = __ldg(fc + 18 * S + self);
+#define LB3D_PULL_LE(Q) d[Q] = __ldg(le_src<Q>(fc, S, c, n, gx, nx, w, Lg, NP));
+  LB3D_PULL_LE(0) LB3D_PULL_LE(1) LB3D_PULL_LE(2) LB3D_PULL_LE(3) LB3D_PULL_LE(4) LB3D_PULL_LE(5)
+  LB3D_PULL_LE(6) LB3D_PULL_LE(7) LB3D_PULL_LE(8) LB3D_PULL_LE(9) LB3D_PULL_LE(10) LB3D_PULL_LE(11)
+  LB3D_PULL_LE(12) LB3D_PULL_LE(13) LB3D_PULL_LE(14) LB3D_PULL_LE(15) LB3D_PULL_LE(16) LB3D_PULL_LE(17)
+#undef LB3D_PULL_LE
+}
+
 // ---------------------------------------------------------------------------
 // The fused kernel.  Grid: persistent CTAs over a tile list.  Populations
 // of lattice L live at f[(c*19+q)*S + L.base + site]; offsets are 32-bit,
@@ -266,7 +302,7 @@ struct FusedGeom {
   static constexpr int SMEM = 16 * (A_F4 + B_F4 + D_F4);
 };
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE, bool LE = false>
 __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * TY) : (TX * TY >= 512 ? 1 : (TX * TY >= 256 ? 2 : 3))))
     k_fused(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
             float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, int S,
@@ -336,12 +372,17 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           Nbr nb;
           make_nbr(nb, gx, gy, gz, nx, ny, nz);
           const int self = noff<18, 1>(nb);
+          LeYZ lw;
+          if constexpr (LE) make_leyz(lw, gy, gz, ny, nz);
           float dr[NC], jm[NC][3];
           float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
             float d[19];
-            pull_comp<ROCK>(F, S, c, nb, self, RK, d);
+            if constexpr (LE)
+              pull_comp_le(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
+            else
+              pull_comp<ROCK>(F, S, c, nb, self, RK, d);
             if (MODE == MODE_MOMENTS) {
               own_moments<1>(d, dr[c], jm[c][0], jm[c][1], jm[c][2]);
             } else {
@@ -583,28 +624,36 @@ size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
 }
 size_t fp32_fused_smem(int nc, const FusedShape &sh) { return fp32_mode_smem(nc, sh, MODE_FUSED); }
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE, bool LE>
 static const void *fused_ptr() {
   if constexpr (MODE == MODE_COLLIDE)
     return (const void *)k_split_collide<NC, TX, TY, ROCK, BODY>;
   else if constexpr (MODE == MODE_COLLIDE2)
-    return (const void *)k_split_collide2<NC, TX, TY, ROCK, BODY>;
+    return (const void *)k_split_collide2<NC, TX, TY, ROCK, BODY, LE>;
   else if constexpr (MODE == MODE_DIPOLE)
     return (const void *)k_split_dipole<TX, TY>;
   else
-    return (const void *)k_fused<NC, TX, TY, ROCK, BODY, MODE>;
+    return (const void *)k_fused<NC, TX, TY, ROCK, BODY, MODE, LE>;
 }
 
-template <int MODE>
+// LE: the Lees-Edwards variants, built for binary lattices without rock and
+// only for the moments and staged collide passes (strategy 2).
+template <int MODE, bool LE = false>
 static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
 #define LB3D_SHAPES(NC, R, B)                                                       \
-  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B, MODE>();         \
-  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B, MODE>();         \
-  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B, MODE>();       \
-  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B, MODE>();         \
-  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B, MODE>();
+  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B, MODE, LE>();     \
+  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B, MODE, LE>();     \
+  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B, MODE, LE>();   \
+  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B, MODE, LE>();     \
+  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B, MODE, LE>();
   // the moments and dipole passes do not apply the body force
   if (MODE == MODE_MOMENTS || MODE == MODE_DIPOLE) body = false;
+  if constexpr (LE) {
+    static_assert(MODE == MODE_MOMENTS || MODE == MODE_COLLIDE2, "no Lees-Edwards variant");
+    if (nc != 2 || rock) return nullptr;
+    if (body) { LB3D_SHAPES(2, false, true) } else { LB3D_SHAPES(2, false, false) }
+    return nullptr;
+  }
   if (MODE == MODE_DIPOLE) rock = false;
   if (nc == 3) {
     if (body) { LB3D_SHAPES(3, false, true) } else { LB3D_SHAPES(3, false, false) }
@@ -620,7 +669,13 @@ static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
   return nullptr;
 }
 
-static const void *kernel_fn(int nc, bool rock, bool body, const FusedShape &sh, int mode) {
+static const void *kernel_fn(int nc, bool rock, bool body, const FusedShape &sh, int mode,
+                             bool le = false) {
+  if (le) {
+    if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS, true>(nc, rock, body, sh);
+    if (mode == MODE_COLLIDE2) return mode_fn<MODE_COLLIDE2, true>(nc, rock, body, sh);
+    return nullptr;
+  }
   if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS>(nc, rock, body, sh);
   if (mode == MODE_COLLIDE) return mode_fn<MODE_COLLIDE>(nc, rock, body, sh);
   if (mode == MODE_DIPOLE) return mode_fn<MODE_DIPOLE>(nc, rock, body, sh);
@@ -682,8 +737,8 @@ static cudaError_t prepare_kernel(const void *fn, int nthreads, size_t smem, int
 static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const FusedShape &sh,
                                const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                                float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
-                               int S, float4 *M, float4 *J, cudaStream_t st) {
-  const void *fn = kernel_fn(nc, rock, body, sh, mode);
+                               int S, float4 *M, float4 *J, cudaStream_t st, bool le = false) {
+  const void *fn = kernel_fn(nc, rock, body, sh, mode, le);
   if (!fn) return cudaErrorInvalidConfiguration;
   size_t smem = fp32_mode_smem(nc, sh, mode);
   int resident = 0;
@@ -717,9 +772,25 @@ static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const Fus
 cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
-                              long long S64, cudaStream_t st, float4 *M, float4 *J) {
+                              long long S64, cudaStream_t st, float4 *M, float4 *J,
+                              const LEStep *le, const DevParams *P) {
   if (S64 * 19 * nc >= (1LL << 31)) return cudaErrorInvalidValue;
   const int S = (int)S64;
+  if (le) {
+    // stage 6 halo, moments pass, stage 8 halo, staged collide pass
+    if (!P || nc != 2 || rock || sh.split != 2 || !M) return cudaErrorInvalidValue;
+    const unsigned g = (unsigned)((P->ny * P->nz + 127) / 128);
+    k_le_pre32<2><<<g, 128, 0, st>>>(*P, *le, d_lat, f0, f1, S);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = launch_mode(MODE_MOMENTS, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1, db0,
+                      db1, rockp, S, M, nullptr, st, true);
+    if (e != cudaSuccess) return e;
+    k_le_post32<2><<<g, 128, 0, st>>>(*P, *le, d_lat, f0, f1, S);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return launch_mode(MODE_COLLIDE2, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1,
+                       db0, db1, rockp, S, M, nullptr, st, true);
+  }
   if (!sh.split)
     return launch_mode(MODE_FUSED, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1, db0,
                        db1, rockp, S, nullptr, nullptr, st);
@@ -802,8 +873,19 @@ LatDesc fp32_make_desc(const DevParams &P, double rho0, long long base, bool roc
 // ---------------------------------------------------------------------------
 long long fp32_footprint(const lb3dc_params &p) {
   const long long N = (long long)p.nx * p.ny * p.nz;
+  const bool le = p.boundary_cond != 0 && (p.inv_fluid == 5 || p.inv_fluid == 6);
+  const long long np = (long long)p.ny * p.nz;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
-         N * (fp32_moment_bytes(p.ncomp) + fp32_own_bytes(p.ncomp)) + 4096;
+         N * (fp32_moment_bytes(p.ncomp) + fp32_own_bytes(p.ncomp)) +
+         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) : 0) + 4096;
+}
+
+// The Lees-Edwards halo planes of a single lattice, referenced by its descriptor.
+static void attach_le(Fp32State &s) {
+  for (int b = 0; b < 2; ++b) {
+    s.lat.le_h[b] = s.le_h[b];
+    s.lat.le_p[b] = s.le_p[b];
+  }
 }
 
 // Shape before any autotuning: the split strategy with the staged collide
@@ -840,6 +922,8 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
 
 int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
   if (!fused_fn(P.nc, false, false, sh)) return LB3DC_EINVAL;
+  // Lees-Edwards lattices run the staged split strategy only
+  if (s.le_h[0] && sh.split != 2) return LB3DC_ENOTSUP;
   if (sh.split && !s.M) return LB3DC_EINVAL;
   if (sh.split < 0 || sh.split > 2) return LB3DC_EINVAL;
   if (sh.zc < 1) return LB3DC_EINVAL;
@@ -854,7 +938,7 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
     if (t[0] > 2 * P.nx && t[0] > 16) continue;
     for (int zc : zcs) {
       if (zc > P.nz && zc != 8) continue;
-      for (int split = 0; split < 3; ++split) out.push_back(FusedShape{t[0], t[1], zc, split});
+      for (int split = P.le ? 2 : 0; split < 3; ++split) out.push_back(FusedShape{t[0], t[1], zc, split});
     }
   }
   return out;
@@ -863,7 +947,7 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
 // The project's autotuner: time each candidate shape with CUDA events on a
 // saved copy of the state, keep the fastest and restore the state.
 int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double *ms_out,
-                  int *ntried, cudaStream_t st) {
+                  int *ntried, cudaStream_t st, const LEStep *le) {
   const size_t pop = (size_t)P.nc * 19 * s.S * sizeof(float);
   const size_t dbs = P.nc == 3 ? 3 * (size_t)s.S * sizeof(float) : 0;
   float *save = nullptr;
@@ -881,10 +965,10 @@ int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double 
   int n = 0;
   for (const FusedShape &sh : fp32_candidate_shapes(P)) {
     if (rebuild_tiles(P, s, sh, st) != LB3DC_OK) continue;
-    if (fp32_run(P, s, rock, 2, st) != LB3DC_OK) continue;
+    if (fp32_run(P, s, rock, 2, st, le) != LB3DC_OK) continue;
     cudaEventRecord(e0, st);
     const int reps = 5;
-    if (fp32_run(P, s, rock, reps, st) != LB3DC_OK) continue;
+    if (fp32_run(P, s, rock, reps, st, le) != LB3DC_OK) continue;
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -930,7 +1014,17 @@ int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStre
   if (cudaMalloc(&s.J, (size_t)N * fp32_own_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
   s.bytes += N * (fp32_moment_bytes(P.nc) + fp32_own_bytes(P.nc));
   if (cudaMalloc(&s.d_lat, sizeof(LatDesc)) != cudaSuccess) return LB3DC_ENOMEM;
+  if (P.le) {
+    const size_t np = (size_t)P.ny * P.nz;
+    for (int b = 0; b < 2; ++b) {
+      if (cudaMalloc(&s.le_h[b], (size_t)P.nc * 19 * np * sizeof(float)) != cudaSuccess ||
+          cudaMalloc(&s.le_p[b], np * sizeof(float2)) != cudaSuccess)
+        return LB3DC_ENOMEM;
+      s.bytes += (long long)(P.nc * 19 * np * sizeof(float) + np * sizeof(float2));
+    }
+  }
   s.lat = fp32_make_desc(P, p.rho0 > 0 ? p.rho0 : 0.7, 0, false);
+  attach_le(s);
   return rebuild_tiles(P, s, default_shape(P), st);
 }
 
@@ -944,6 +1038,12 @@ void fp32_free(Fp32State &s) {
   if (s.d_tiles) cudaFree(s.d_tiles);
   if (s.M) cudaFree(s.M);
   if (s.J) cudaFree(s.J);
+  for (int b = 0; b < 2; ++b) {
+    if (s.le_h[b]) cudaFree(s.le_h[b]);
+    if (s.le_p[b]) cudaFree(s.le_p[b]);
+    s.le_h[b] = nullptr;
+    s.le_p[b] = nullptr;
+  }
   s.d_lat = nullptr;
   s.d_tiles = nullptr;
   s.M = nullptr;
@@ -961,7 +1061,9 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   bool any = false;
   for (long long i = 0; i < N; ++i) any |= rk[i] != 0;
   if (any && P.nc == 3) return LB3DC_EINVAL;
+  if (any && P.le) return LB3DC_ENOTSUP;  // the FP32 Lees-Edwards kernels have no walls
   s.lat = fp32_make_desc(P, rho0, 0, any);
+  attach_le(s);
   s.lat.parity = 0;
   // FP64 staging on the device, converted to deviations by a kernel
   double *dn = nullptr;
@@ -1062,20 +1164,27 @@ int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, doubl
   return LB3DC_OK;
 }
 
-int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_t st) {
-  return fp32_run(P, s, rock, 1, st);
+int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_t st,
+              const LEStep *le) {
+  return fp32_run(P, s, rock, 1, st, le);
 }
 
-int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st) {
+int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st,
+             const LEStep *le) {
   FusedShape sh{s.tx, s.ty, s.zc, s.split};
   const bool rk = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
+  if (le && !s.le_h[0]) return LB3DC_ESTATE;
+  // kernels per step: the pass(es), two Lees-Edwards halo kernels, the parity flip
+  const int passes = sh.split ? (P.nc == 3 ? 3 : 2) : 1;
+  const int per_step = passes + (le ? 2 : 0) + 1;
   for (int i = 0; i < nsteps; ++i) {
     if (s.timer) s.timer->start(st);
     cudaError_t e = fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, 0,
-                                      s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M, s.J);
+                                      s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M, s.J,
+                                      le, &P);
     if (s.timer) {
       s.timer->stop(st);
-      s.timer->launches += 2;
+      s.timer->launches += per_step;
     }
     if (e != cudaSuccess) return LB3DC_ECUDA;
     e = fp32_flip_parity(s.d_lat, 1, st);

@@ -25,6 +25,12 @@ struct LatDesc {
   float g_accn, g_accn_x, g_accn_y;
   int amin_x, amax_x, amin_y, amax_y, amin_z, amax_z, inv_fluid;
   float rho0, psi0, em0;  // psi(rho0) = 1 - exp(-rho0), em0 = exp(-rho0)
+  // Lees-Edwards x-halo planes (binary single lattices; null otherwise):
+  // le_h[0/1] the sheared pre-stream populations below x = 0 / above
+  // x = nx - 1, [nc][19][nz][ny] deviations; le_p[0/1] the psi deviations of
+  // the post-stream halo sites, [nz][ny] float2 {dpsi_r, dpsi_b}.
+  float *le_h[2];
+  float2 *le_p[2];
 };
 constexpr int LAT_ROCK = 1, LAT_BODY = 2, LAT_ACTIVE = 4;
 
@@ -50,6 +56,8 @@ struct Fp32State {
   int grid = 0;
   long long bytes = 0;
   KernelTimer *timer = nullptr;  // optional, owned by the handle
+  float *le_h[2] = {nullptr, nullptr};  // Lees-Edwards halo planes (see LatDesc)
+  float2 *le_p[2] = {nullptr, nullptr};
 };
 
 // Launch configuration of the fused kernel.
@@ -68,8 +76,13 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
 int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, double *n,
                   double *db, double *rho, double *mom, double *da, const uint8_t *rock,
                   cudaStream_t st);
-int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_t st);
-int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st);
+// One step; le gives this step's Lees-Edwards offset (null: periodic).
+int fp32_step(const DevParams &P, Fp32State &s, const uint8_t *rock, cudaStream_t st,
+              const LEStep *le = nullptr);
+// nsteps steps; le (null: periodic) is applied unchanged to every step, as the
+// autotuner wants; a Lees-Edwards time loop advances one step at a time.
+int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, cudaStream_t st,
+             const LEStep *le = nullptr);
 int fp32_dump(const DevParams &P, Fp32State &s, int field, const uint8_t *rock, double *out,
               cudaStream_t st);
 cudaError_t fp32_reduce_conservation(const DevParams &P, Fp32State &s, const uint8_t *rock,
@@ -83,11 +96,16 @@ void fp32_tiles_for(const LatDesc &L, int lat_id, const FusedShape &sh, std::vec
 // fin/fout select by parity inside the kernel; `flip` is applied by caller.
 // Each pass runs as many CTAs as are resident at once for that kernel (at
 // most ntiles); max_grid > 0 caps that number.
+// With le (a binary single lattice whose LatDesc carries the halo planes,
+// strategy 2 only) the step also builds the sheared x-halos: the stage-6
+// populations before the moments pass and the stage-8 psi planes before the
+// collide pass.
 cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh,
                               const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
                               long long S, cudaStream_t st, float4 *M = nullptr,
-                              float4 *J = nullptr);
+                              float4 *J = nullptr, const LEStep *le = nullptr,
+                              const DevParams *P = nullptr);
 // Bytes per site of the split strategy's moment fields.
 inline long long fp32_moment_bytes(int nc) { return nc == 3 ? 32 : 8; }
 inline long long fp32_own_bytes(int nc) { return nc == 3 ? 48 : 32; }
@@ -98,7 +116,7 @@ int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaS
 // Candidate shapes of the autotuner.
 std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P);
 int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double *ms_out,
-                  int *ntried, cudaStream_t st);
+                  int *ntried, cudaStream_t st, const LEStep *le = nullptr);
 int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh);
 
 }  // namespace lb3d

@@ -280,7 +280,22 @@ __device__ __forceinline__ void pull_async(const float *__restrict__ F, int S, i
 #undef LB3D_APULL
 }
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY>
+// pull_async with the Lees-Edwards halo planes across the x boundary
+template <int NT>
+__device__ __forceinline__ void pull_async_le(const float *__restrict__ F, int S, int c, const Nbr &n,
+                                              int self, int gx, int nx, const LeYZ &w,
+                                              const LatDesc &Lg, int NP, float *stage) {
+  const float *fc = F + c * 19 * S;
+  cp_async4(stage + 18 * NT, fc + 18 * S + self);
+#define LB3D_APULL_LE(Q) cp_async4(stage + (Q) * NT, le_src<Q>(fc, S, c, n, gx, nx, w, Lg, NP));
+  LB3D_APULL_LE(0) LB3D_APULL_LE(1) LB3D_APULL_LE(2) LB3D_APULL_LE(3) LB3D_APULL_LE(4)
+  LB3D_APULL_LE(5) LB3D_APULL_LE(6) LB3D_APULL_LE(7) LB3D_APULL_LE(8) LB3D_APULL_LE(9)
+  LB3D_APULL_LE(10) LB3D_APULL_LE(11) LB3D_APULL_LE(12) LB3D_APULL_LE(13) LB3D_APULL_LE(14)
+  LB3D_APULL_LE(15) LB3D_APULL_LE(16) LB3D_APULL_LE(17)
+#undef LB3D_APULL_LE
+}
+
+template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false>
 __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
     k_split_collide2(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                      float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
@@ -327,6 +342,10 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
           cp_async4(b, DBn + i);
           cp_async4(b + 1, DBn + S + i);
           cp_async4(b + 2, DBn + 2 * S + i);
+        } else if (LE && vx == -1) {  // sheared halo below x = 0
+          cp_async8(ringP2 + sl + s, Lg.le_p[0] + iy + ny * gz);
+        } else if (LE && vx == nx) {  // sheared halo above x = nx - 1
+          cp_async8(ringP2 + sl + s, Lg.le_p[1] + iy + ny * gz);
         } else {
           cp_async8(ringP2 + sl + s, reinterpret_cast<const float2 *>(Mb) + i);
         }
@@ -336,11 +355,20 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
     auto issue_pulls = [&](int k) -> bool {
       if (!act) return true;
       Nbr nb;
-      make_nbr(nb, gx, gy, pmod(z0 + k, nz), nx, ny, nz);
+      const int gz = pmod(z0 + k, nz);
+      make_nbr(nb, gx, gy, gz, nx, ny, nz);
       const int self = noff<18, 1>(nb);
       if (ROCK && __ldg(RK + self) != 0) return true;
+      if constexpr (LE) {
+        LeYZ lw;
+        make_leyz(lw, gy, gz, ny, nz);
 #pragma unroll
-      for (int c = 0; c < NC; ++c) pull_async<ROCK, NT>(F, S, c, nb, self, RK, mystage + c * 19 * NT);
+        for (int c = 0; c < NC; ++c)
+          pull_async_le<NT>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, mystage + c * 19 * NT);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) pull_async<ROCK, NT>(F, S, c, nb, self, RK, mystage + c * 19 * NT);
+      }
       return false;
     };
 
@@ -463,4 +491,121 @@ __global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
     cp_async_wait<0>();
     __syncthreads();  // the next tile refills ring slots 0..2
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// Lees-Edwards x-halos of the FP32 path (binary single lattices), one
+// thread per (y, z), in FP64 from the FP32 deviations with the FP64 path's
+// adjustment (le_adjust: the equilibrium shift by -/+ 2 shear_u along z,
+// the clipping rule and the top halo's reading of the adjusted bottom site,
+// code/lb3d_bc_leesedwards.F90:147-1315).
+//   k_le_pre32  (stage 6): pre-stream populations at x = nx - 1 / x = 0,
+//               interpolated between z + e, z + e + 1 / z - e - 1, z - e,
+//               written to le_h[0/1] as deviations; the pulls across the
+//               x boundary read them.
+//   k_le_post32 (stage 8): the same for the post-stream populations (each
+//               pulled as the moments pass pulls it), reduced to the halo
+//               densities and written to le_p[0/1] as psi deviations; the
+//               collide pass's force stencil reads them.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double wq64(int q) { return q == 18 ? 1.0 / 3.0 : 1.0 / 36.0; }
+
+template <int NC>
+__global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ lat,
+                           const float *__restrict__ f0, const float *__restrict__ f1, int S) {
+  const LatDesc &Lg = *lat;
+  const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NP) return;
+  const int y = t % ny, z = t / ny;
+  const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base;
+  const double rho0 = (double)Lg.rho0, f = L.lefrac;
+  double hb[NC][19], ht[NC][19];
+  {
+    const int ia = (nx - 1) + nx * (y + ny * pmod(z + L.eoff, nz));
+    const int ib = (nx - 1) + nx * (y + ny * pmod(z + L.eoff + 1, nz));
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q) {
+        const double w = __dmul_rn(wq64(q), rho0);
+        hb[c][q] = (1.0 - f) * ((double)F[(c * 19 + q) * S + ia] + w) +
+                   f * ((double)F[(c * 19 + q) * S + ib] + w);
+      }
+    le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
+  }
+  {
+    const int ia = nx * (y + ny * pmod(z - L.eoff - 1, nz));
+    const int ib = nx * (y + ny * pmod(z - L.eoff, nz));
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q) {
+        const double w = __dmul_rn(wq64(q), rho0);
+        ht[c][q] = f * ((double)F[(c * 19 + q) * S + ia] + w) +
+                   (1.0 - f) * ((double)F[(c * 19 + q) * S + ib] + w);
+      }
+    le_adjust<NC>(P, ht, hb, L.shear_u, +1.0);
+  }
+  for (int c = 0; c < NC; ++c)
+    for (int q = 0; q < 19; ++q) {
+      const double w = __dmul_rn(wq64(q), rho0);
+      Lg.le_h[0][(c * 19 + q) * NP + t] = (float)(hb[c][q] - w);
+      Lg.le_h[1][(c * 19 + q) * NP + t] = (float)(ht[c][q] - w);
+    }
+}
+
+template <int NC>
+__global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ lat,
+                            const float *__restrict__ f0, const float *__restrict__ f1, int S) {
+  const LatDesc &Lg = *lat;
+  const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NP) return;
+  const int y = t % ny, z = t / ny;
+  const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base;
+  const double rho0 = (double)Lg.rho0, f = L.lefrac;
+  // post-stream population q of component c at (x, yy, zz)
+  auto post = [&](int c, int q, int x, int yy, int zz) -> double {
+    float v;
+    if (q == 18) {
+      v = F[(c * 19 + 18) * S + x + nx * (yy + ny * zz)];
+    } else {
+      const int xu = x - cx(q), yu = pmod(yy - cy(q), ny), zu = pmod(zz - cz(q), nz);
+      if (xu < 0)
+        v = Lg.le_h[0][(c * 19 + q) * NP + yu + ny * zu];
+      else if (xu >= nx)
+        v = Lg.le_h[1][(c * 19 + q) * NP + yu + ny * zu];
+      else
+        v = F[(c * 19 + q) * S + xu + nx * (yu + ny * zu)];
+    }
+    return (double)v + __dmul_rn(wq64(q), rho0);
+  };
+  double hb[NC][19], ht[NC][19];
+  {
+    const int za = pmod(z + L.eoff, nz), zb = pmod(z + L.eoff + 1, nz);
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q)
+        hb[c][q] = (1.0 - f) * post(c, q, nx - 1, y, za) + f * post(c, q, nx - 1, y, zb);
+    le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
+  }
+  {
+    const int za = pmod(z - L.eoff - 1, nz), zb = pmod(z - L.eoff, nz);
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q)
+        ht[c][q] = f * post(c, q, 0, y, za) + (1.0 - f) * post(c, q, 0, y, zb);
+    le_adjust<NC>(P, ht, hb, L.shear_u, +1.0);
+  }
+  double dl[NC], dh[NC];
+  const double em0 = exp(-rho0);
+  for (int c = 0; c < NC; ++c) {
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      a = a + hb[c][q] * (double)gw(q);
+      b = b + ht[c][q] * (double)gw(q);
+    }
+    // psi(rho) - psi(rho0) = -e^{-rho0} expm1(-(rho - rho0))
+    dl[c] = -em0 * expm1(-(a - rho0));
+    dh[c] = -em0 * expm1(-(b - rho0));
+  }
+  Lg.le_p[0][t] = make_float2((float)dl[0], (float)dl[1]);
+  Lg.le_p[1][t] = make_float2((float)dh[0], (float)dh[1]);
 }

@@ -142,3 +142,50 @@ def test_staged_collide_equals_plain_split(nc, dims, shape, rock):
     assert np.array_equal(out[0]["n"], out[1]["n"])
     if nc == 3:
         assert np.array_equal(out[0]["db"], out[1]["db"])
+
+
+def test_fp32_lees_edwards_reference_case():
+    """The reference's leesEdwards system through the FP32 path: sheared
+    x-halos built in FP64 from the FP32 state each step; the plane offset
+    (shear_sum) is host FP64 bookkeeping and equals the oracle's exactly."""
+    p, st = load_case("leesEdwards")
+    lat, a, b, o = run_both(p, st, 20)
+    check(a, b, p.ncomp, "leesEdwards")
+    assert lat.lees_edwards[0] == o.shear_sum
+
+
+@pytest.mark.parametrize("shear_u,omega", [(0.05, 0.0), (-0.3, 0.0), (0.2, 0.31)])
+@pytest.mark.parametrize("dims", [(40, 12, 20), (8, 6, 10)])
+def test_fp32_lees_edwards_offsets(dims, shear_u, omega):
+    """Positive, negative (lelo < 0) and oscillating plane offsets; lattices
+    wider than one tile (the halo columns sit in the first and last tile) and
+    narrower than one tile."""
+    p = _params(dims, 2, boundary_cond=-1, inv_fluid=5, shear_u=shear_u, shear_omega=omega,
+                g_accn_x=1e-5)
+    st = uniform_mixture(*dims, 2, seed=5)
+    st["shear_sum"] = 0.37
+    from lb3d_b200.lib import Lattice
+    lat = Lattice(p, precision=1)
+    lat.upload_state(st)
+    o = Oracle(p, st)
+    for _ in range(2):
+        lat.time_loop(10)
+        o.run(10)
+        check(lat.download(), o.get(), 2, f"LE {dims} shear_u={shear_u}")
+    assert lat.lees_edwards[0] == o.shear_sum
+
+
+def test_fp32_lees_edwards_limits():
+    """The FP32 Lees-Edwards kernels have no walls and exist for the staged
+    split strategy only; both limits are reported, not run."""
+    from lb3d_b200.lib import Lattice, Lb3dError
+    p = _params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=5, shear_u=0.05)
+    st = uniform_mixture(16, 8, 8, 2, seed=1)
+    lat = Lattice(p, precision=1)
+    lat.upload_state(st)
+    with pytest.raises(Lb3dError):
+        lat.set_launch_shape(32, 8, 16, 1)
+    st["rock"] = np.zeros((8, 8, 16))
+    st["rock"][0, 0, 0] = 1.0
+    with pytest.raises(Lb3dError):
+        Lattice(p, precision=1).upload_state(st)
