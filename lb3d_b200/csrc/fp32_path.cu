@@ -608,7 +608,7 @@ constexpr int MODE_DIPOLE = 3, MODE_COLLIDE2 = 4;
 size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
   const size_t AN1 = (size_t)(sh.tx + 2) * (sh.ty + 2);
   if (mode == MODE_DIPOLE) return 16 * 5 * AN1 + (size_t)4 * 5 * sh.tx * sh.ty;
-  if (mode == MODE_COLLIDE2)
+  if (mode == MODE_COLLIDE2)  // Collide2Geom: ring slots x entry bytes + population stage
     return 5 * AN1 * (nc == 3 ? 32 : 8) + (size_t)19 * nc * sh.tx * sh.ty * 4;
   if (mode == MODE_COLLIDE) return 16 * 3 * AN1 * (nc == 3 ? 2 : 1);
   const int H = mode == MODE_MOMENTS ? 0 : (nc == 3 ? 2 : 1);

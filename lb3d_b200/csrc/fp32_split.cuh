@@ -250,9 +250,13 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
 // Shared-memory layout of k_split_collide2 (bytes): psi ring [5][AN] float4
 // (float2 for binary), dipole ring [5][AN] float4 (ternary), population
 // stage [19*NC][NT] float.
+// Five ring slots (one barrier per plane).  Three CTAs of 128 threads per
+// SM (at most 168 registers) measured faster than four CTAs at 128 registers
+// with a four-slot ring and a second barrier per plane.
 template <int NC, int TX, int TY>
 struct Collide2Geom {
-  static constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2), RS = 5;
+  static constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2);
+  static constexpr int RS = 5, MINB = NT >= 256 ? 2 : 3;
   static constexpr int PB = (NC == 3) ? 16 : 8;  // psi entry bytes
   static constexpr int P_BYTES = RS * AN * PB;
   static constexpr int B_BYTES = (NC == 3) ? RS * AN * 16 : 0;
@@ -296,7 +300,7 @@ __device__ __forceinline__ void pull_async_le(const float *__restrict__ F, int S
 }
 
 template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false>
-__global__ void __launch_bounds__(TX *TY, (TX * TY >= 256 ? 2 : 3))
+__global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
     k_split_collide2(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                      float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
                      int S, const float4 *__restrict__ Mf) {

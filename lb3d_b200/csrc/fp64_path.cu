@@ -99,7 +99,11 @@ __global__ void k_le_halo(DevParams P, LEStep S, const double *__restrict__ src,
 // flux and the post-stream moments (code/lb3d_advection.F90:54-151,
 // code/lb3d_bc_bounce.F90:53-90, code/lb3d_analysis.F90:64-102).
 // ---------------------------------------------------------------------------
-template <int NC, bool LE>
+// One launch per component c (components are independent here; the
+// advected dipole flux uses the surfactant only), which keeps one
+// component's 19 pulls live per thread; FLUX marks the surfactant launch,
+// which also accumulates the dipole flux.
+template <int NC, bool LE, bool FLUX>
 __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__restrict__ fin,
                                                 double *__restrict__ fout, double *__restrict__ rho,
                                                 double *__restrict__ psi, double *__restrict__ mom,
@@ -107,7 +111,7 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
                                                 const double *__restrict__ db,
                                                 const uint8_t *__restrict__ rock,
                                                 const double *__restrict__ hlo,
-                                                const double *__restrict__ hhi) {
+                                                const double *__restrict__ hhi, int c) {
   const long long N = P.nsites;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -146,9 +150,7 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
   };
 
   double d0 = 0.0, d1 = 0.0, d2 = 0.0;
-  // one component at a time keeps 19 pulls live, not 19*NC
-#pragma unroll 1
-  for (int c = 0; c < NC; ++c) {
+  {
     double n[19];
 #pragma unroll
     for (int q = 0; q < 18; ++q) {
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
         n[q] = fin[(c * 19 + q) * N + i];
     }
     n[REST] = fin[(c * 19 + REST) * N + i];
-    if (NC == 3 && c == 2) {
+    if (FLUX) {
       // advected dipole flux: bounce-back terms first (lb3d_bc_bounce_back_hw
       // runs before lb3d_advection_step), then the pulls, then the rest
       // population (code/lb3d_advection.F90:137-148).
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
     mom[(c * 3 + 1) * N + i] = u1;
     mom[(c * 3 + 2) * N + i] = u2;
   }
-  if (NC == 3) {
+  if (FLUX) {
     da[i] = d0;
     da[N + i] = d1;
     da[2 * N + i] = d2;
@@ -594,15 +596,21 @@ cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, dou
                         const uint8_t *rock, const double *hlo, const double *hhi,
                         cudaStream_t st) {
   unsigned gr = grid_for(P.nsites, 256);
-  if (P.nc == 2) {
-    if (P.le)
-      k_stream<2, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi);
-    else
-      k_stream<2, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi);
-  } else {
-    k_stream<3, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi);
+  for (int c = 0; c < P.nc; ++c) {
+    if (P.nc == 2) {
+      if (P.le)
+        k_stream<2, true, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+      else
+        k_stream<2, false, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+    } else if (c < 2) {
+      k_stream<3, false, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+    } else {
+      k_stream<3, false, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
   }
-  return cudaGetLastError();
+  return cudaSuccess;
 }
 
 cudaError_t fp64_dipole(const DevParams &P, const double *rho, const double *da, double *db,
