@@ -178,6 +178,16 @@ int lb3dc_get_timestep(const lb3dc_handle *h, int *nt);
 int lb3dc_reduce_conservation(lb3dc_handle *h, double mass[3], double mom[3]);
 /* Counts non-finite and negative populations (code/lb3d_sanity.F90:79-130). */
 int lb3dc_sanity(lb3dc_handle *h, long long *n_nonfinite, long long *n_negative);
+/* The velocity statistics of lbe_sanity_check (code/lb3d_sanity.F90:130-371):
+ * for each species s and axis k (index 3*s + k), over fluid sites where
+ * |rho_s| > 1e-12 with v = (sum_i n_i g_i c_i) amass_s / rho_s: maxvel = the
+ * maximum |v_k|, maxpos = its site (1-based x, y, z; ties go to the site the
+ * reference's x-outer, z-inner loop visits last; 0,0,0 when no site
+ * qualifies), velsum = the sum of v_k (divide by the site count for the
+ * reference's average), n_too_fast = sites where some species has
+ * |v| > 0.1, n_fluid = fluid sites.  Any output may be NULL. */
+int lb3dc_sanity_velocity(lb3dc_handle *h, double maxvel[9], int maxpos[27], double velsum[9],
+                          long long *n_fluid, long long *n_too_fast);
 /* Science dump fields at the current state (code/lb3d_io_dump_data.F90):
  * "od", "wd", "sur", "vel", "rock" -> [site]; "dir", "arr" -> [site][3];
  * FP64 values, site index x fastest. */

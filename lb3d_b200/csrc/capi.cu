@@ -91,6 +91,19 @@ int dalloc(lb3dc_handle *h, T **ptr, size_t count) {
   return 0;
 }
 
+// Clears the populations (ncq arrays of n sites) and, when given, the
+// dipole arrays of rock sites.
+__global__ void k_clear_rock(double *f, int ncq, double *db, double *da, const uint8_t *rock,
+                             long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || rock[i] == 0) return;
+  for (int cq = 0; cq < ncq; ++cq) f[cq * n + i] = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    if (db) db[k * n + i] = 0.0;
+    if (da) da[k * n + i] = 0.0;
+  }
+}
+
 int validate(const lb3dc_params *p, std::string &why) {
   if (!p) return (why = "params is NULL", LB3DC_EINVAL);
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return (why = "lattice sizes must be >= 1", LB3DC_EINVAL);
@@ -331,31 +344,29 @@ int lb3dc_upload_state(lb3dc_handle *h, const double *n, const double *db, const
   cudaSetDevice(h->device);
   const size_t N = (size_t)h->P.nsites, nc = (size_t)h->p.ncomp;
   // lbe_init_rock_colour (code/lb3d_ic_rock.F90:146-189): populations and
-  // dipoles of rock sites are cleared.
-  std::vector<double> nn(n, n + nc * 19 * N);
-  std::vector<double> dd;
-  if (nc == 3) dd.assign(db, db + 3 * N);
+  // dipoles of rock sites are cleared -- on the device, so the caller's
+  // (possibly pinned) arrays are copied as they are.
   std::vector<uint8_t> rk(N, 0);
+  bool any = false;
   if (rock)
-    for (size_t i = 0; i < N; ++i) {
-      if (rock[i] != 0.0) {
-        rk[i] = 1;
-        for (size_t cq = 0; cq < nc * 19; ++cq) nn[cq * N + i] = 0.0;
-        if (nc == 3)
-          for (int k = 0; k < 3; ++k) dd[(size_t)k * N + i] = 0.0;
-      }
-    }
+    for (size_t i = 0; i < N; ++i)
+      if (rock[i] != 0.0) rk[i] = 1, any = true;
   CK(h, cudaMemcpyAsync(h->rock, rk.data(), N, cudaMemcpyHostToDevice, h->stream));
   if (h->p.precision == LB3DC_FP64) {
-    CK(h, cudaMemcpyAsync(h->f, nn.data(), nc * 19 * N * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->f, n, nc * 19 * N * 8, cudaMemcpyHostToDevice, h->stream));
     if (nc == 3) {
-      CK(h, cudaMemcpyAsync(h->db, dd.data(), 3 * N * 8, cudaMemcpyHostToDevice, h->stream));
-      CK(h, cudaMemcpyAsync(h->da, dd.data(), 3 * N * 8, cudaMemcpyHostToDevice, h->stream));
+      CK(h, cudaMemcpyAsync(h->db, db, 3 * N * 8, cudaMemcpyHostToDevice, h->stream));
+      CK(h, cudaMemcpyAsync(h->da, db, 3 * N * 8, cudaMemcpyHostToDevice, h->stream));
+    }
+    if (any) {
+      k_clear_rock<<<(unsigned)((N + 255) / 256), 256, 0, h->stream>>>(
+          h->f, (int)(nc * 19), nc == 3 ? h->db : nullptr, nc == 3 ? h->da : nullptr, h->rock,
+          (long long)N);
+      CK(h, cudaGetLastError());
     }
     CK(h, fp64_moments(h->P, h->f, h->rho, h->psi, h->mom, h->stream));
   } else {
-    int rc = fp32_upload(h->P, h->p, h->s32, nn.data(), nc == 3 ? dd.data() : nullptr, h->rock,
-                         h->stream);
+    int rc = fp32_upload(h->P, h->p, h->s32, n, nc == 3 ? db : nullptr, h->rock, h->stream);
     if (rc) return fail(h, rc, "FP32 upload failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   CK(h, cudaStreamSynchronize(h->stream));
@@ -658,6 +669,30 @@ int lb3dc_sanity(lb3dc_handle *h, long long *n_nonfinite, long long *n_negative)
   if (n_nonfinite) *n_nonfinite = (long long)cnt[0];
   if (n_negative) *n_negative = (long long)cnt[1];
   return cnt[0] ? fail(h, LB3DC_ENAN, "%llu non-finite populations", cnt[0]) : LB3DC_OK;
+}
+
+int lb3dc_sanity_velocity(lb3dc_handle *h, double maxvel[9], int maxpos[27], double velsum[9],
+                          long long *n_fluid, long long *n_too_fast) {
+  int rc = need_loaded(h);
+  if (rc) return rc;
+  rc = ensure_scratch(h, reduce_scratch_bytes(h->P.nsites));
+  if (rc) return rc;
+  SanityVelocity v;
+  cudaError_t e;
+  if (h->p.precision == LB3DC_FP64)
+    e = sanity_velocity_fp64(h->P, h->f, h->rock, h->scratch, v, h->stream);
+  else
+    e = fp32_sanity_velocity(h->P, h->s32, h->rock, h->scratch, v, h->stream);
+  CK(h, e);
+  for (int k = 0; k < 9; ++k) {
+    if (maxvel) maxvel[k] = v.vmax[k];
+    if (velsum) velsum[k] = v.vsum[k];
+    if (maxpos)
+      for (int a = 0; a < 3; ++a) maxpos[3 * k + a] = v.pos[k][a];
+  }
+  if (n_fluid) *n_fluid = v.n_fluid;
+  if (n_too_fast) *n_too_fast = v.n_too_fast;
+  return LB3DC_OK;
 }
 
 int lb3dc_dump(lb3dc_handle *h, const char *field, double *out) {

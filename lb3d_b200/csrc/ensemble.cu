@@ -47,8 +47,10 @@ struct lb3dc_ensemble {
   int max_lat = 0, tile_cap = 0, ntiles = 0, grid = 0;
   std::vector<Member> members;
   std::map<long long, long long> free_ranges;  // base -> length
-  FusedShape shape{16, 8, 16, 1};
+  FusedShape shape{16, 8, 8, 2};
   float4 *M = nullptr, *J = nullptr;
+  double *stage = nullptr;  // FP64 staging of one member's populations (admit / retire)
+  size_t stage_bytes = 0;
   bool dirty = true;  // tile list must be rebuilt
   bool body = false;
   cudaGraph_t graph = nullptr;
@@ -65,6 +67,17 @@ int efail(lb3dc_ensemble *e, int code, const std::string &m) {
   if (e) e->err = m;
   else set_global_error(code, m.c_str());
   return code;
+}
+
+// Device staging for a member's FP64 populations, grown on demand and kept.
+bool ensure_stage(lb3dc_ensemble *e, size_t bytes) {
+  if (e->stage_bytes >= bytes) return true;
+  if (e->stage) cudaFree(e->stage);
+  e->stage = nullptr;
+  e->stage_bytes = 0;
+  if (cudaMalloc(&e->stage, bytes) != cudaSuccess) return false;
+  e->stage_bytes = bytes;
+  return true;
 }
 
 void drop_graph(lb3dc_ensemble *e) {
@@ -298,6 +311,7 @@ int lb3dc_ensemble_destroy(lb3dc_ensemble *e) {
   if (e->J) cudaFree(e->J);
   if (e->d_lat) cudaFree(e->d_lat);
   if (e->d_tiles) cudaFree(e->d_tiles);
+  if (e->stage) cudaFree(e->stage);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return LB3DC_OK;
@@ -333,17 +347,13 @@ int lb3dc_ensemble_admit(lb3dc_ensemble *e, const lb3dc_params *p, const double 
   Member &m = e->members[slot];
   const long long N = m.n;
   const double rho0 = m.desc.rho0;
-  // deviations into the parity-0 buffer's range
-  std::vector<float> h((size_t)e->nc * 19 * N);
-  for (int c = 0; c < e->nc; ++c)
-    for (int q = 0; q < 19; ++q) {
-      const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
-      for (long long i = 0; i < N; ++i) h[((size_t)c * 19 + q) * N + i] = (float)(n[((size_t)c * 19 + q) * N + i] - w);
-    }
-  for (int c = 0; c < e->nc * 19; ++c)
-    if (cudaMemcpyAsync(e->f[0] + (size_t)c * e->S + base, h.data() + (size_t)c * N, N * 4,
-                        cudaMemcpyHostToDevice, e->stream) != cudaSuccess)
-      return efail(e, LB3DC_ECUDA, "upload failed");
+  // FP64 populations to the device, converted there into deviations in the
+  // parity-0 buffer's range
+  const size_t nb = (size_t)e->nc * 19 * N * sizeof(double);
+  if (!ensure_stage(e, nb)) return efail(e, LB3DC_ENOMEM, "staging allocation failed");
+  if (cudaMemcpyAsync(e->stage, n, nb, cudaMemcpyHostToDevice, e->stream) != cudaSuccess ||
+      fp32_from_fp64(e->stage, e->f[0], e->S, base, N, e->nc, rho0, nullptr, e->stream) != cudaSuccess)
+    return efail(e, LB3DC_ECUDA, "upload failed");
   if (e->nc == 3) {
     std::vector<float> d(3 * N);
     for (long long i = 0; i < 3 * N; ++i) d[i] = (float)db[i];
@@ -455,18 +465,14 @@ int lb3dc_ensemble_retire(lb3dc_ensemble *e, int slot, double *n, double *db) {
   const int cur = m.desc.parity;
   cudaStreamSynchronize(e->stream);
   if (n) {
-    std::vector<float> h((size_t)e->nc * 19 * N);
-    for (int c = 0; c < e->nc * 19; ++c)
-      cudaMemcpyAsync(h.data() + (size_t)c * N, e->f[cur] + (size_t)c * e->S + m.base, N * 4,
-                      cudaMemcpyDeviceToHost, e->stream);
-    if (cudaStreamSynchronize(e->stream) != cudaSuccess) return efail(e, LB3DC_ECUDA, "download failed");
-    const double rho0 = m.desc.rho0;
-    for (int c = 0; c < e->nc; ++c)
-      for (int q = 0; q < 19; ++q) {
-        const double w = (q == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
-        for (long long i = 0; i < N; ++i)
-          n[((size_t)c * 19 + q) * N + i] = (double)h[((size_t)c * 19 + q) * N + i] + w;
-      }
+    // deviations -> FP64 populations on the device, one copy back
+    const size_t nb = (size_t)e->nc * 19 * N * sizeof(double);
+    if (!ensure_stage(e, nb)) return efail(e, LB3DC_ENOMEM, "staging allocation failed");
+    if (fp32_to_fp64(e->f[cur], e->stage, e->S, m.base, N, e->nc, m.desc.rho0, e->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(n, e->stage, nb, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess)
+      return efail(e, LB3DC_ECUDA, "download failed");
   }
   if (db && e->nc == 3) {
     std::vector<float> d(3 * N);

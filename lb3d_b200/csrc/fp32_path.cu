@@ -584,21 +584,39 @@ __global__ void k_to_fp64(const float *__restrict__ f, double *__restrict__ n, l
                     __dmul_rn(q == 18 ? 1.0 / 3.0 : 1.0 / 36.0, rho0));
 }
 
-// FP64 populations -> FP32 deviations (upload); rock sites keep n = 0.
+// FP64 populations -> FP32 deviations (upload); rock sites (rock[i] != 0,
+// when rock is given) hold n = 0.
 __global__ void k_from_fp64(const double *__restrict__ n, float *__restrict__ f, long long S,
-                            long long base, long long N, int nc, double rho0) {
+                            long long base, long long N, int nc, double rho0,
+                            const uint8_t *__restrict__ rock = nullptr) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  const bool solid = rock && rock[i] != 0;
   for (int c = 0; c < nc; ++c)
     for (int q = 0; q < 19; ++q) {
       const double w = __dmul_rn(q == 18 ? 1.0 / 3.0 : 1.0 / 36.0, rho0);
-      f[((long long)c * 19 + q) * S + base + i] = (float)__dsub_rn(n[((long long)c * 19 + q) * N + i], w);
+      const double v = solid ? 0.0 : n[((long long)c * 19 + q) * N + i];
+      f[((long long)c * 19 + q) * S + base + i] = (float)__dsub_rn(v, w);
     }
 }
 
 }  // namespace f32
 
 using namespace f32;
+
+cudaError_t fp32_to_fp64(const float *f, double *out, long long S, long long base, long long N,
+                         int nc, double rho0, cudaStream_t st) {
+  if (N <= 0) return cudaSuccess;
+  k_to_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(f, out, S, base, N, nc, rho0);
+  return cudaGetLastError();
+}
+
+cudaError_t fp32_from_fp64(const double *n, float *f, long long S, long long base, long long N,
+                           int nc, double rho0, const uint8_t *rock, cudaStream_t st) {
+  if (N <= 0) return cudaSuccess;
+  k_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(n, f, S, base, N, nc, rho0, rock);
+  return cudaGetLastError();
+}
 
 // ---------------------------------------------------------------------------
 // launch table
@@ -1071,13 +1089,15 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   if (cudaMalloc(&dn, nb) != cudaSuccess) return LB3DC_ENOMEM;
   cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, st);
   for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-    k_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dn, s.f[b], s.S, 0, N, P.nc, rho0);
+    k_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dn, s.f[b], s.S, 0, N, P.nc, rho0,
+                                                             any ? rockp : nullptr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cudaFree(dn);
   if (e != cudaSuccess) return LB3DC_ECUDA;
   if (P.nc == 3) {
+    // (ternary lattices have no rock: refused above)
     std::vector<float> d(3 * N);
     for (long long i = 0; i < 3 * N; ++i) d[i] = (float)db[i];
     for (int b = 0; b < 2; ++b)
@@ -1230,45 +1250,19 @@ int fp32_dump(const DevParams &P, Fp32State &s, int field, const uint8_t *rock, 
 cudaError_t fp32_reduce_conservation(const DevParams &P, Fp32State &s, const uint8_t *rock,
                                      double *scratch, double mass[3], double mom[3],
                                      cudaStream_t st) {
-  // Download-based FP64 sums (reduction over the host copy in FP64).
-  const long long N = P.nsites;
-  std::vector<double> n((size_t)P.nc * 19 * N);
-  lb3dc_params dummy{};
-  int rc = fp32_download(P, dummy, s, n.data(), nullptr, nullptr, nullptr, nullptr, rock, st);
-  (void)scratch;
-  if (rc) return cudaErrorUnknown;
-  std::vector<uint8_t> rk(N);
-  cudaMemcpyAsync(rk.data(), rock, N, cudaMemcpyDeviceToHost, st);
-  cudaStreamSynchronize(st);
-  for (int k = 0; k < 3; ++k) mass[k] = mom[k] = 0.0;
-  for (long long i = 0; i < N; ++i) {
-    if (rk[i]) continue;
-    for (int c = 0; c < P.nc; ++c)
-      for (int q = 0; q < 19; ++q) {
-        double ng = n[((size_t)c * 19 + q) * N + i] * gw(q);
-        mass[c] += ng;
-        mom[0] += ng * cx(q);
-        mom[1] += ng * cy(q);
-        mom[2] += ng * cz(q);
-      }
-  }
-  return cudaSuccess;
+  return reduce_conservation_fp32(P, s.f[s.lat.parity], s.S, 0, (double)s.lat.rho0, rock, scratch,
+                                  mass, mom, st);
 }
 
 cudaError_t fp32_sanity_counts(const DevParams &P, Fp32State &s, unsigned long long *scratch,
                                unsigned long long cnt[2], cudaStream_t st) {
-  (void)scratch;
-  const long long N = P.nsites;
-  std::vector<double> n((size_t)P.nc * 19 * N);
-  lb3dc_params dummy{};
-  if (fp32_download(P, dummy, s, n.data(), nullptr, nullptr, nullptr, nullptr, nullptr, st))
-    return cudaErrorUnknown;
-  cnt[0] = cnt[1] = 0;
-  for (double v : n) {
-    if (!std::isfinite(v)) ++cnt[0];
-    else if (v < 0) ++cnt[1];
-  }
-  return cudaSuccess;
+  return sanity_counts_fp32(P, s.f[s.lat.parity], s.S, 0, (double)s.lat.rho0, scratch, cnt, st);
+}
+
+cudaError_t fp32_sanity_velocity(const DevParams &P, Fp32State &s, const uint8_t *rock,
+                                 void *scratch, SanityVelocity &out, cudaStream_t st) {
+  return sanity_velocity_fp32(P, s.f[s.lat.parity], s.S, 0, (double)s.lat.rho0, rock, scratch, out,
+                              st);
 }
 
 }  // namespace lb3d

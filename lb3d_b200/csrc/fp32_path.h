@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "reduce.h"
 
 namespace lb3d {
 
@@ -90,6 +91,8 @@ cudaError_t fp32_reduce_conservation(const DevParams &P, Fp32State &s, const uin
                                      cudaStream_t st);
 cudaError_t fp32_sanity_counts(const DevParams &P, Fp32State &s, unsigned long long *scratch,
                                unsigned long long cnt[2], cudaStream_t st);
+cudaError_t fp32_sanity_velocity(const DevParams &P, Fp32State &s, const uint8_t *rock,
+                                 void *scratch, SanityVelocity &out, cudaStream_t st);
 
 // Shared with the ensemble runtime: tile list for a lattice, fused launch.
 void fp32_tiles_for(const LatDesc &L, int lat_id, const FusedShape &sh, std::vector<Tile> &out);
@@ -106,6 +109,13 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
                               long long S, cudaStream_t st, float4 *M = nullptr,
                               float4 *J = nullptr, const LEStep *le = nullptr,
                               const DevParams *P = nullptr);
+// FP32 deviations <-> FP64 populations of one lattice (N sites at `base`
+// in arrays of stride S), on the device; rock (optional, device, N bytes)
+// marks sites whose populations are zero.
+cudaError_t fp32_to_fp64(const float *f, double *out, long long S, long long base, long long N,
+                         int nc, double rho0, cudaStream_t st);
+cudaError_t fp32_from_fp64(const double *n, float *f, long long S, long long base, long long N,
+                           int nc, double rho0, const uint8_t *rock, cudaStream_t st);
 // Bytes per site of the split strategy's moment fields.
 inline long long fp32_moment_bytes(int nc) { return nc == 3 ? 32 : 8; }
 inline long long fp32_own_bytes(int nc) { return nc == 3 ? 48 : 32; }

@@ -82,6 +82,7 @@ def lib():
         "lb3dc_get_timestep": (I, [H, ctypes.POINTER(I)]),
         "lb3dc_reduce_conservation": (I, [H, _D, _D]),
         "lb3dc_sanity": (I, [H, ctypes.POINTER(LL), ctypes.POINTER(LL)]),
+        "lb3dc_sanity_velocity": (I, [H, _D, ctypes.POINTER(I), _D, ctypes.POINTER(LL), ctypes.POINTER(LL)]),
         "lb3dc_dump": (I, [H, ctypes.c_char_p, _D]),
         "lb3dc_xdr_read_checkpoint": (I, [ctypes.c_char_p, I, I, I, I, _D, _D, _D]),
         "lb3dc_xdr_write_checkpoint": (I, [ctypes.c_char_p, I, I, I, I, _D, _D, _D, _D]),
@@ -281,6 +282,22 @@ class Lattice:
         if rc not in (0, LB3DC_ENAN):
             self._ck(rc)
         return a.value, b.value
+
+
+    def sanity_velocity(self):
+        """lbe_sanity_check's velocity statistics: dict with maxvel [species][axis],
+        maxpos [species][axis][xyz] (1-based), velsum [species][axis], n_fluid,
+        n_too_fast (sites with some species' |v| > 0.1)."""
+        return _sanity_velocity(lib().lb3dc_sanity_velocity, self.h, self._ck)
+
+
+def _sanity_velocity(fn, h, check):
+    mv, vs = np.zeros(9), np.zeros(9)
+    mp = (ctypes.c_int * 27)()
+    nf, nt = ctypes.c_longlong(), ctypes.c_longlong()
+    check(fn(h, ptr(mv), mp, ptr(vs), ctypes.byref(nf), ctypes.byref(nt)))
+    return dict(maxvel=mv.reshape(3, 3), maxpos=np.array(mp[:], dtype=np.int64).reshape(3, 3, 3),
+                velsum=vs.reshape(3, 3), n_fluid=nf.value, n_too_fast=nt.value)
 
 
 def footprint(params: Params) -> int:

@@ -857,6 +857,59 @@ int lb3do_sums(const void *h, double mass[3], double mom[3]) {
   return 0;
 }
 
+// lbe_sanity_check's velocity statistics, code/lb3d_sanity.F90:130-229: the
+// reference's x-outer, z-inner loop over fluid sites; per species with
+// |rho| > 1e-12 the velocity sum(n g c) amass / rho, the running maximum of
+// each |v_k| taken with `>=` (ties move to the later site), the sum of v_k,
+// and the sites where some species has norm(v) > 0.1.
+int lb3do_sanity_velocity(const void *h, double maxvel[9], int maxpos[27], double velsum[9],
+                          long long *n_fluid, long long *n_too_fast) {
+  const Oracle *o = static_cast<const Oracle *>(h);
+  const double small = 1.0e-12, max_vel = 0.1;
+  for (int k = 0; k < 9; ++k) {
+    maxvel[k] = 0.0;
+    velsum[k] = 0.0;
+    for (int a = 0; a < 3; ++a) maxpos[3 * k + a] = 0;
+  }
+  long long fs = 0, tf = 0;
+  for (int x = 1; x <= o->nx; ++x)
+    for (int y = 1; y <= o->ny; ++y)
+      for (int z = 1; z <= o->nz; ++z) {
+        const Site &s = o->N[o->idx(x, y, z)];
+        if (s.rock != 0.0) continue;
+        ++fs;
+        bool fast = false;
+        for (int c = 0; c < o->nc; ++c) {
+          double r = 0.0, m[3] = {0, 0, 0};
+          for (int q = 0; q < 19; ++q) {
+            const double ng = s.n[c][q] * (double)G[q];
+            r = r + ng;
+            m[0] = m[0] + ng * CX[q];
+            m[1] = m[1] + ng * CY[q];
+            m[2] = m[2] + ng * CZ[q];
+          }
+          if (std::fabs(r) > small) {
+            double v[3];
+            for (int k = 0; k < 3; ++k) v[k] = m[k] * o->amass[c] / r;
+            for (int k = 0; k < 3; ++k) {
+              velsum[3 * c + k] = velsum[3 * c + k] + v[k];
+              if (std::fabs(v[k]) >= maxvel[3 * c + k]) {
+                maxvel[3 * c + k] = std::fabs(v[k]);
+                maxpos[9 * c + 3 * k] = x;
+                maxpos[9 * c + 3 * k + 1] = y;
+                maxpos[9 * c + 3 * k + 2] = z;
+              }
+            }
+            if (std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) > max_vel) fast = true;
+          }
+        }
+        if (fast) ++tf;
+      }
+  if (n_fluid) *n_fluid = fs;
+  if (n_too_fast) *n_too_fast = tf;
+  return 0;
+}
+
 double lb3do_shear_sum(const void *h) { return static_cast<const Oracle *>(h)->shear_sum; }
 int lb3do_nt(const void *h) { return static_cast<const Oracle *>(h)->nt; }
 

@@ -74,6 +74,10 @@ int lb3do_dump(void *h, const char *field, double *out);
 
 /* Sum over fluid sites of rho_c and of the momentum sum_c u_c. */
 int lb3do_sums(const void *h, double mass[3], double mom[3]);
+/* Velocity statistics of lbe_sanity_check (code/lb3d_sanity.F90:130-229),
+ * index 3*species + axis; positions 1-based x, y, z. */
+int lb3do_sanity_velocity(const void *h, double maxvel[9], int maxpos[27], double velsum[9],
+                          long long *n_fluid, long long *n_too_fast);
 
 double lb3do_shear_sum(const void *h);
 int lb3do_nt(const void *h);

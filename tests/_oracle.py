@@ -35,6 +35,9 @@ def lib():
         L.lb3do_get.argtypes = [V, D, D, D, D, D]
         L.lb3do_dump.argtypes = [V, ctypes.c_char_p, D]
         L.lb3do_sums.argtypes = [V, D, D]
+        L.lb3do_sanity_velocity.argtypes = [V, D, ctypes.POINTER(ctypes.c_int), D,
+                                            ctypes.POINTER(ctypes.c_longlong),
+                                            ctypes.POINTER(ctypes.c_longlong)]
         L.lb3do_shear_sum.argtypes = [V]
         L.lb3do_shear_sum.restype = ctypes.c_double
         L.lb3do_nt.argtypes = [V]
@@ -116,6 +119,10 @@ class Oracle:
         u = np.zeros(3)
         lib().lb3do_sums(self.h, _ptr(m), _ptr(u))
         return m, u
+
+    def sanity_velocity(self):
+        from lb3d_b200.lib import _sanity_velocity
+        return _sanity_velocity(lib().lb3do_sanity_velocity, self.h, lambda rc: None)
 
     @property
     def shear_sum(self):

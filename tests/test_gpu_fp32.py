@@ -189,3 +189,18 @@ def test_fp32_lees_edwards_limits():
     st["rock"][0, 0, 0] = 1.0
     with pytest.raises(Lb3dError):
         Lattice(p, precision=1).upload_state(st)
+
+
+def test_fp32_sanity_velocity_and_sums_on_device():
+    """The FP32 path's sanity statistics and conservation sums are reduced on
+    the device from the deviations; against the FP64 oracle after 10 steps."""
+    p, st = load_case("gyroid")
+    lat, a, b, o = run_both(p, st, 10)
+    va, vb = lat.sanity_velocity(), o.sanity_velocity()
+    np.testing.assert_allclose(va["maxvel"], vb["maxvel"], rtol=0, atol=2e-6)
+    np.testing.assert_allclose(va["velsum"], vb["velsum"], rtol=0, atol=1e-3)
+    assert va["n_fluid"] == vb["n_fluid"]
+    m, u = lat.conservation()
+    mo, uo = o.sums()
+    np.testing.assert_allclose(m, mo, rtol=2e-6)
+    assert lat.sanity() == (0, 0)

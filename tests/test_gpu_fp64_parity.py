@@ -208,3 +208,45 @@ def test_error_paths():
         lat.time_loop(1)  # no state loaded
     with pytest.raises(Lb3dError):
         lat.bc_apply(7)
+
+
+@pytest.mark.parametrize("case", ["gyroid", "wettingWall", "bodyForce"])
+def test_sanity_velocity_matches_oracle(case):
+    """lbe_sanity_check's velocity statistics on the device: the maxima and
+    their sites equal the reference loop's exactly, the velocity sums to
+    FP64 rounding (a tree sum against the reference's running sum)."""
+    p, st = load_case(case)
+    lat = _lattice(p, st)
+    o = Oracle(p, st)
+    lat.time_loop(5)
+    o.run(5)
+    a, b = lat.sanity_velocity(), o.sanity_velocity()
+    np.testing.assert_array_equal(a["maxvel"], b["maxvel"])
+    np.testing.assert_array_equal(a["maxpos"], b["maxpos"])
+    np.testing.assert_allclose(a["velsum"], b["velsum"], rtol=1e-11, atol=1e-12)
+    assert (a["n_fluid"], a["n_too_fast"]) == (b["n_fluid"], b["n_too_fast"])
+
+
+def test_sanity_velocity_ties_and_fast_sites():
+    """With only rest populations every velocity is exactly zero: the maxima
+    tie everywhere and the reported site is the last one of the reference's
+    loop.  Then a few sites are given large momenta and counted as too fast."""
+    p = _params((9, 7, 5), 2)
+    st = uniform_mixture(9, 7, 5, 2, seed=2)
+    st["n"][:, 18] = st["n"].sum(axis=1)  # all mass at rest
+    st["n"][:, :18] = 0.0
+    lat = _lattice(p, st)
+    o = Oracle(p, st)
+    a, b = lat.sanity_velocity(), o.sanity_velocity()
+    np.testing.assert_array_equal(a["maxpos"], b["maxpos"])
+    assert tuple(a["maxpos"][0, 0]) == (9, 7, 5)
+    assert a["n_too_fast"] == 0
+    st2 = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    st2["n"][0, 0, 1, 2, 3] += 0.2   # +x population of red at (x=4, y=3, z=2)
+    st2["n"][1, 4, 3, 5, 6] += 0.3   # +z population of blue at (x=7, y=6, z=4)
+    lat2 = _lattice(p, st2)
+    o2 = Oracle(p, st2)
+    a, b = lat2.sanity_velocity(), o2.sanity_velocity()
+    np.testing.assert_array_equal(a["maxvel"], b["maxvel"])
+    np.testing.assert_array_equal(a["maxpos"], b["maxpos"])
+    assert a["n_too_fast"] == b["n_too_fast"] == 2
