@@ -172,6 +172,7 @@ DevParams make_dev_params(const lb3dc_params &p) {
   P.rc_r = p.rock_colour_r > 0 ? p.rock_colour_r : 0.0;
   P.rc_b = p.rock_colour_b > 0 ? p.rock_colour_b : 0.0;
   P.le = (p.boundary_cond != 0 && (p.inv_fluid == 5 || p.inv_fluid == 6)) ? 1 : 0;
+  P.any_rock = 1;  // until a state without rock is uploaded
   return P;
 }
 
@@ -352,6 +353,7 @@ int lb3dc_upload_state(lb3dc_handle *h, const double *n, const double *db, const
     for (size_t i = 0; i < N; ++i)
       if (rock[i] != 0.0) rk[i] = 1, any = true;
   CK(h, cudaMemcpyAsync(h->rock, rk.data(), N, cudaMemcpyHostToDevice, h->stream));
+  h->P.any_rock = any ? 1 : 0;
   if (h->p.precision == LB3DC_FP64) {
     CK(h, cudaMemcpyAsync(h->f, n, nc * 19 * N * 8, cudaMemcpyHostToDevice, h->stream));
     if (nc == 3) {

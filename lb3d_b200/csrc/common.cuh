@@ -46,6 +46,7 @@ struct DevParams {
   int inv_fluid;
   double rc_r, rc_b;  // rock colour at rock sites (0 where not set)
   int le;             // Lees-Edwards on the x-planes
+  int any_rock;       // some site is rock (0: the stream kernel skips the rock tests)
 };
 
 // Per-step Lees-Edwards values, computed on the host in FP64 exactly as

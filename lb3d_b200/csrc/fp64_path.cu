@@ -103,7 +103,7 @@ __global__ void k_le_halo(DevParams P, LEStep S, const double *__restrict__ src,
 // advected dipole flux uses the surfactant only), which keeps one
 // component's 19 pulls live per thread; FLUX marks the surfactant launch,
 // which also accumulates the dipole flux.
-template <int NC, bool LE, bool FLUX>
+template <int NC, bool LE, bool FLUX, bool ROCK>
 __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__restrict__ fin,
                                                 double *__restrict__ fout, double *__restrict__ rho,
                                                 double *__restrict__ psi, double *__restrict__ mom,
@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   int x, y, z;
   site_xyz(i, nx, ny, x, y, z);
-  const bool fluid = rock[i] == 0;
+  // without rock every site is fluid and the pulls do not wait on rock loads
+  const bool fluid = !ROCK || rock[i] == 0;
   const long long NP = (long long)ny * nz;
 
   // upstream site of each moving direction (32-bit: the FP64 path bounds a
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
       upf[q] = true;
     } else {
       up[q] = (int)sidx(wrap(xu, nx), yu, zu, nx, ny);
-      upf[q] = rock[up[q]] == 0;
+      upf[q] = !ROCK || rock[up[q]] == 0;
     }
   }
   auto pulled = [&](int c, int q) -> double {
@@ -165,14 +166,16 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
       // runs before lb3d_advection_step), then the pulls, then the rest
       // population (code/lb3d_advection.F90:137-148).
       if (fluid) {
+        if (ROCK) {
 #pragma unroll
-        for (int s = 0; s < 18; ++s) {
-          long long ja = sidx(wrap(x + cx(s), nx), wrap(y + cy(s), ny), wrap(z + cz(s), nz), nx, ny);
-          if (rock[ja] != 0) {
-            double ng = fin[(2 * 19 + s) * N + i] * (double)gw(s);
-            d0 = d0 + ng * db[ja];
-            d1 = d1 + ng * db[N + ja];
-            d2 = d2 + ng * db[2 * N + ja];
+          for (int s = 0; s < 18; ++s) {
+            long long ja = sidx(wrap(x + cx(s), nx), wrap(y + cy(s), ny), wrap(z + cz(s), nz), nx, ny);
+            if (rock[ja] != 0) {
+              double ng = fin[(2 * 19 + s) * N + i] * (double)gw(s);
+              d0 = d0 + ng * db[ja];
+              d1 = d1 + ng * db[N + ja];
+              d2 = d2 + ng * db[2 * N + ja];
+            }
           }
         }
 #pragma unroll
@@ -596,20 +599,26 @@ cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, dou
                         const uint8_t *rock, const double *hlo, const double *hhi,
                         cudaStream_t st) {
   unsigned gr = grid_for(P.nsites, 256);
+#define LB3D_STREAM(NC_, LE_, FLUX_)                                                           \
+  (P.any_rock ? k_stream<NC_, LE_, FLUX_, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, \
+                                                                    db, rock, hlo, hhi, c)        \
+              : k_stream<NC_, LE_, FLUX_, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, \
+                                                                     db, rock, hlo, hhi, c))
   for (int c = 0; c < P.nc; ++c) {
     if (P.nc == 2) {
       if (P.le)
-        k_stream<2, true, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+        LB3D_STREAM(2, true, false);
       else
-        k_stream<2, false, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+        LB3D_STREAM(2, false, false);
     } else if (c < 2) {
-      k_stream<3, false, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+      LB3D_STREAM(3, false, false);
     } else {
-      k_stream<3, false, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, da, db, rock, hlo, hhi, c);
+      LB3D_STREAM(3, false, true);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+#undef LB3D_STREAM
   return cudaSuccess;
 }
 

@@ -106,7 +106,8 @@ extern "C" int lb3dc_time_loop_fp64_noalloc(const lb3dc_params *p, double *f, do
     if (e != cudaSuccess) return err(LB3DC_ECUDA, cudaGetErrorString(e));
     rk = zero;
   }
-  const lb3d::DevParams P = lb3d::dev_params_from(*p);
+  lb3d::DevParams P = lb3d::dev_params_from(*p);
+  P.any_rock = rock ? 1 : 0;  // a caller's mask may hold rock
   for (int s = 0; s < nsteps; ++s) {
     // Every scratch field is written by the stream kernel before the dipole
     // and collide kernels read it, so nothing else needs clearing.
