@@ -168,6 +168,10 @@ class Params:
     rock_colour_b: float = 0.0
     bdist: int = 0
     restore: int = 0
+    inv_type: int = 0
+    pr: float = 0.5
+    pg: float = 0.1
+    pb: float = 1.0
     # product-only fields (not in the reference's namelists)
     precision: int = 0  # 0: FP64 plain drop-in, 1: FP32 deviation storage
     rho0: float = 0.7  # reference density of the FP32 deviation storage
@@ -216,7 +220,8 @@ class Params:
             raise ValueError("only the bdist = 2 equilibrium is implemented")
         if self.psifunc != 2:
             raise ValueError("only psifunc = 2 (psi = 1 - exp(-rho)) is implemented")
-        if self.boundary_cond != 0 and self.inv_fluid >= 0 and not self.lees_edwards:
+        if (self.boundary_cond != 0 and self.inv_fluid >= 0 and not self.lees_edwards
+                and self.inv_fluid != 12):
             raise ValueError("invasion boundaries (inv_fluid=%d) are not implemented" % self.inv_fluid)
         if self.boundary_cond > 0:
             raise ValueError("boundary_cond > 0 (generated walls) is not implemented")
@@ -284,6 +289,8 @@ _C_FIELDS = [
     ("boundary_cond", ctypes.c_int), ("inv_fluid", ctypes.c_int),
     ("rock_colour_r", ctypes.c_double), ("rock_colour_b", ctypes.c_double),
     ("bdist", ctypes.c_int), ("restore", ctypes.c_int),
+    ("inv_type", ctypes.c_int), ("pr", ctypes.c_double), ("pg", ctypes.c_double),
+    ("pb", ctypes.c_double),
 ]
 
 

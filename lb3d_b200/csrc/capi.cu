@@ -114,7 +114,14 @@ int validate(const lb3dc_params *p, std::string &why) {
   bool le = p->boundary_cond != 0 && (p->inv_fluid == 5 || p->inv_fluid == 6);
   if (p->ncomp == 3 && le)
     return (why = "FATAL: Lees Edwards BC are not supported for ternary mixtures", LB3DC_EINVAL);
-  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le)
+  const bool zouhe = p->boundary_cond != 0 && p->inv_fluid == 12;
+  if (zouhe && p->precision != LB3DC_FP64)
+    return (why = "Zou-He flux boundaries run on the FP64 path", LB3DC_ENOTSUP);
+  if (zouhe && p->nz < 2)
+    return (why = "the Zou-He flux boundaries need two distinct z planes (nz >= 2)", LB3DC_EINVAL);
+  if (zouhe && p->inv_type != 0 && p->inv_type != 1 && p->inv_type != -1)
+    return (why = "inv_type must be 0, 1 or -1 for the Zou-He flux boundaries", LB3DC_EINVAL);
+  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && !zouhe)
     return (why = "invasion boundaries are not implemented", LB3DC_ENOTSUP);
   if (p->boundary_cond > 0) return (why = "boundary_cond > 0 is not implemented", LB3DC_ENOTSUP);
   if (p->tau_r <= 0 || p->tau_b <= 0 || (p->ncomp == 3 && (p->tau_s <= 0 || p->tau_d <= 0)))
@@ -173,6 +180,11 @@ DevParams make_dev_params(const lb3dc_params &p) {
   P.rc_b = p.rock_colour_b > 0 ? p.rock_colour_b : 0.0;
   P.le = (p.boundary_cond != 0 && (p.inv_fluid == 5 || p.inv_fluid == 6)) ? 1 : 0;
   P.any_rock = 1;  // until a state without rock is uploaded
+  P.zouhe = (p.boundary_cond != 0 && p.inv_fluid == 12) ? 1 : 0;
+  P.inv_type = p.inv_type;
+  P.zh_uz[0] = p.pr;
+  P.zh_uz[1] = p.pb;
+  P.zh_uz[2] = p.pg;
   return P;
 }
 
@@ -491,6 +503,11 @@ int lb3dc_bc_apply(lb3dc_handle *h, int stage) {
     return LB3DC_OK;
   }
   if (stage == 8) {
+    if (h->P.zouhe && h->p.precision == LB3DC_FP64) {
+      // code/lb3d_bc.F90:125-133: the invasion boundaries come first
+      CK(h, fp64_zouhe_flux(h->P, h->g, h->da, h->db, h->rock, h->stream));
+      h->timer.launches += 1;
+    }
     if (h->le && h->p.precision == LB3DC_FP64) {
       CK(h, fp64_le_halo(h->P, le_step(h), h->g, nullptr, nullptr, h->rlo, h->rhi, h->plo,
                          h->phi, h->stream));

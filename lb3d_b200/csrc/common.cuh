@@ -47,6 +47,9 @@ struct DevParams {
   double rc_r, rc_b;  // rock colour at rock sites (0 where not set)
   int le;             // Lees-Edwards on the x-planes
   int any_rock;       // some site is rock (0: the stream kernel skips the rock tests)
+  int zouhe;          // Zou-He flux boundaries on the z planes (inv_fluid 12)
+  int inv_type;       // their closure: 0, 1 or -1 (flux / density)
+  double zh_uz[3];    // their inflow per component: red pr, blue pb, surfactant pg
 };
 
 // Per-step Lees-Edwards values, computed on the host in FP64 exactly as

@@ -221,6 +221,106 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
 }
 
 // ---------------------------------------------------------------------------
+// Zou-He flux boundaries, code/lb3d_invasion.F90:2143-2457 (one rank: both
+// z planes are boundary planes).  One thread per site of the z = 1 and
+// z = nz planes; per component (surfactant, red, blue) the populations
+// entering the lattice are closed from the known ones and the inflow uz
+// (divided by the density for inv_type < 0), in the expression order of
+// the reference; the surfactant's advected dipole flux is recomputed from
+// its new populations and the dipoles of the upstream sites (periodic
+// images across the planes, as the stage-6 halo holds them).  Densities
+// and velocities keep their advection values, as in the reference.
+// F(i) is the reference's 1-based direction i.
+// ---------------------------------------------------------------------------
+__device__ void zouhe_flux_site(double *Fp, double uz, bool bottom, int itype) {
+  auto F = [&](int i) -> double & { return Fp[i - 1]; };
+  const double ux = 0., uy = 0.;
+  double rho;
+  if (bottom) {
+    if (itype < 0) {
+      rho = F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+            2. * (F(6) + F(10) + F(14) + F(16) + F(18)) + uz;
+      uz = (rho > 0.) ? uz / rho : 0.;
+    } else {
+      rho = (F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+             2. * (F(6) + F(10) + F(14) + F(16) + F(18))) /
+            (1. - uz);
+    }
+    F(5) = F(6) + uz * rho / 3.;
+    if (itype == 0) {
+      F(15) = F(18) - (F(3) - F(4)) / 4. + rho * uz / 6.;
+      F(17) = F(16) + (F(3) - F(4)) / 4. + rho * uz / 6.;
+      F(9) = F(14) - (F(1) - F(2)) / 4. + rho * uz / 6.;
+      F(13) = F(10) + (F(1) - F(2)) / 4. + rho * uz / 6.;
+    } else if (itype == 1 || itype == -1) {
+      F(15) = F(18) - (F(7) + F(11) + F(3) - F(8) - F(12) - F(4)) / 2. + uz * rho / 6. + uy * rho / 2.;
+      F(17) = F(16) - (F(8) + F(12) + F(4) - F(7) - F(11) - F(3)) / 2. + uz * rho / 6. - uy * rho / 2.;
+      F(9) = F(14) - (F(7) + F(8) + F(1) - F(11) - F(12) - F(2)) / 2. + uz * rho / 6. + ux * rho / 2.;
+      F(13) = F(10) - (F(11) + F(12) + F(2) - F(7) - F(8) - F(1)) / 2. + uz * rho / 6. - ux * rho / 2.;
+    }
+  } else {
+    if (itype < 0) {
+      rho = F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+            2. * (F(5) + F(9) + F(13) + F(15) + F(17)) - uz;
+      uz = (rho > 0.) ? uz / rho : 0.;
+    } else {
+      rho = (F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+             2. * (F(5) + F(9) + F(13) + F(15) + F(17))) /
+            (uz + 1.);
+    }
+    F(6) = F(5) - uz * rho / 3.;
+    if (itype == 0) {
+      F(18) = F(15) + (F(3) - F(4)) / 4. - rho * uz / 6.;
+      F(16) = F(17) - (F(3) - F(4)) / 4. - rho * uz / 6.;
+      F(14) = F(9) + (F(1) - F(2)) / 4. - rho * uz / 6.;
+      F(10) = F(13) - (F(1) - F(2)) / 4. - rho * uz / 6.;
+    } else if (itype == 1 || itype == -1) {
+      F(18) = F(15) + (F(7) + F(11) + F(3) - F(8) - F(12) - F(4)) / 2. - uz * rho / 6. - uy * rho / 2.;
+      F(16) = F(17) + (F(8) + F(12) + F(4) - F(7) - F(11) - F(3)) / 2. - uz * rho / 6. + uy * rho / 2.;
+      F(14) = F(9) + (F(7) + F(8) + F(1) - F(11) - F(12) - F(2)) / 2. - uz * rho / 6. - ux * rho / 2.;
+      F(10) = F(13) + (F(11) + F(12) + F(2) - F(7) - F(8) - F(1)) / 2. - uz * rho / 6. + ux * rho / 2.;
+    }
+  }
+}
+
+template <int NC>
+__global__ void k_zouhe_flux(DevParams P, double *__restrict__ g, double *__restrict__ da,
+                             const double *__restrict__ db, const uint8_t *__restrict__ rock) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const long long N = P.nsites;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * nx * ny) return;
+  const bool bottom = t < nx * ny;
+  const int xy = bottom ? t : t - nx * ny;
+  const int x = xy % nx, y = xy / nx, z = bottom ? 0 : nz - 1;
+  const long long i = sidx(x, y, z, nx, ny);
+  if (rock[i] != 0) return;
+  const int order[3] = {2, 0, 1};  // surfactant, red, blue
+  for (int k = 0; k < 3; ++k) {
+    const int c = order[k];
+    if (c >= NC) continue;
+    double F[19];
+    for (int q = 0; q < 19; ++q) F[q] = g[(c * 19 + q) * N + i] * (double)gw(q);
+    zouhe_flux_site(F, P.zh_uz[c], bottom, P.inv_type);
+    for (int q = 0; q < 19; ++q) g[(c * 19 + q) * N + i] = F[q] / (double)gw(q);
+    if (NC == 3 && c == 2) {
+      double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+      for (int q = 0; q < 19; ++q) {
+        const long long j =
+            sidx(wrap(x - cx(q), nx), wrap(y - cy(q), ny), wrap(z - cz(q), nz), nx, ny);
+        const double ng = g[(2 * 19 + q) * N + i] * (double)gw(q);
+        d0 = d0 + ng * db[j];
+        d1 = d1 + ng * db[N + j];
+        d2 = d2 + ng * db[2 * N + j];
+      }
+      da[i] = d0;
+      da[N + i] = d1;
+      da[2 * N + i] = d2;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Dipole relaxation, code/lb3d_collision.F90:296-403 (ternary, periodic).
 // Reads rho and da of the 18 neighbours; writes db in place (no neighbour
 // reads db in this pass).
@@ -591,6 +691,16 @@ cudaError_t fp64_le_halo(const DevParams &P, const LEStep &S, const double *src,
     k_le_halo<2><<<grid_for(n, 128), 128, 0, st>>>(P, S, src, hlo, hhi, rlo, rhi, plo, phi);
   else
     k_le_halo<3><<<grid_for(n, 128), 128, 0, st>>>(P, S, src, hlo, hhi, rlo, rhi, plo, phi);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_zouhe_flux(const DevParams &P, double *g, double *da, const double *db,
+                            const uint8_t *rock, cudaStream_t st) {
+  const int n = 2 * P.nx * P.ny;
+  if (P.nc == 2)
+    k_zouhe_flux<2><<<grid_for(n, 128), 128, 0, st>>>(P, g, da, db, rock);
+  else
+    k_zouhe_flux<3><<<grid_for(n, 128), 128, 0, st>>>(P, g, da, db, rock);
   return cudaGetLastError();
 }
 

@@ -9,6 +9,10 @@ namespace lb3d {
 cudaError_t fp64_le_halo(const DevParams &P, const LEStep &S, const double *src, double *hlo,
                          double *hhi, double *rlo, double *rhi, double *plo, double *phi,
                          cudaStream_t st);
+// Zou-He flux boundaries on the z = 1 and z = nz planes (inv_fluid 12),
+// applied to the post-stream populations g and the advected dipole flux da.
+cudaError_t fp64_zouhe_flux(const DevParams &P, double *g, double *da, const double *db,
+                            const uint8_t *rock, cudaStream_t st);
 cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, double *rho,
                         double *psi, double *mom, double *da, const double *db,
                         const uint8_t *rock, const double *hlo, const double *hhi,

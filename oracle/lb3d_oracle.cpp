@@ -561,6 +561,102 @@ struct Oracle {
         }
   }
 
+  // ---- Zou-He flux boundaries, code/lb3d_invasion.F90:2143-2457 ---------
+  // lbe_invade_zouandheflux on one rank (both z planes are boundary
+  // planes), applied to the post-stream populations at stage 8 before the
+  // halo exchange.  Per fluid site of the plane and per component (the
+  // surfactant first, then red, then blue): with F = n g, the unknown
+  // populations entering the lattice are closed from the known ones and
+  // the prescribed inflow uz (a velocity, or a flux divided by the density
+  // for inv_type < 0), n = F / g; the surfactant's advected dipole flux is
+  // then recomputed from its new populations.  Densities and velocities
+  // keep their advection values (the reference recomputes them only for
+  // Lees-Edwards).  F(i) below is the reference's 1-based direction i.
+  void zouhe_flux_site(double *Fp, double uz, bool bottom, int itype) {
+    auto F = [&](int i) -> double & { return Fp[i - 1]; };
+    const double ux = 0., uy = 0.;
+    double rho;
+    if (bottom) {
+      if (itype < 0) {
+        rho = F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+              2. * (F(6) + F(10) + F(14) + F(16) + F(18)) + uz;
+        if (rho > 0.)
+          uz = uz / rho;
+        else
+          uz = 0.;
+      } else {
+        rho = (F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+               2. * (F(6) + F(10) + F(14) + F(16) + F(18))) /
+              (1. - uz);
+      }
+      F(5) = F(6) + uz * rho / 3.;
+      if (itype == 0) {
+        F(15) = F(18) - (F(3) - F(4)) / 4. + rho * uz / 6.;
+        F(17) = F(16) + (F(3) - F(4)) / 4. + rho * uz / 6.;
+        F(9) = F(14) - (F(1) - F(2)) / 4. + rho * uz / 6.;
+        F(13) = F(10) + (F(1) - F(2)) / 4. + rho * uz / 6.;
+      } else if (itype == 1 || itype == -1) {
+        F(15) = F(18) - (F(7) + F(11) + F(3) - F(8) - F(12) - F(4)) / 2. + uz * rho / 6. + uy * rho / 2.;
+        F(17) = F(16) - (F(8) + F(12) + F(4) - F(7) - F(11) - F(3)) / 2. + uz * rho / 6. - uy * rho / 2.;
+        F(9) = F(14) - (F(7) + F(8) + F(1) - F(11) - F(12) - F(2)) / 2. + uz * rho / 6. + ux * rho / 2.;
+        F(13) = F(10) - (F(11) + F(12) + F(2) - F(7) - F(8) - F(1)) / 2. + uz * rho / 6. - ux * rho / 2.;
+      }
+    } else {
+      if (itype < 0) {
+        rho = F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+              2. * (F(5) + F(9) + F(13) + F(15) + F(17)) - uz;
+        if (rho > 0.)
+          uz = uz / rho;
+        else
+          uz = 0.;
+      } else {
+        rho = (F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
+               2. * (F(5) + F(9) + F(13) + F(15) + F(17))) /
+              (uz + 1.);
+      }
+      F(6) = F(5) - uz * rho / 3.;
+      if (itype == 0) {
+        F(18) = F(15) + (F(3) - F(4)) / 4. - rho * uz / 6.;
+        F(16) = F(17) - (F(3) - F(4)) / 4. - rho * uz / 6.;
+        F(14) = F(9) + (F(1) - F(2)) / 4. - rho * uz / 6.;
+        F(10) = F(13) - (F(1) - F(2)) / 4. - rho * uz / 6.;
+      } else if (itype == 1 || itype == -1) {
+        F(18) = F(15) + (F(7) + F(11) + F(3) - F(8) - F(12) - F(4)) / 2. - uz * rho / 6. - uy * rho / 2.;
+        F(16) = F(17) + (F(8) + F(12) + F(4) - F(7) - F(11) - F(3)) / 2. - uz * rho / 6. + uy * rho / 2.;
+        F(14) = F(9) + (F(7) + F(8) + F(1) - F(11) - F(12) - F(2)) / 2. - uz * rho / 6. - ux * rho / 2.;
+        F(10) = F(13) + (F(11) + F(12) + F(2) - F(7) - F(8) - F(1)) / 2. - uz * rho / 6. + ux * rho / 2.;
+      }
+    }
+  }
+  void invade_zouhe_flux() {
+    // inflow per component: red pr, blue pb, surfactant pg
+    const double uzc[3] = {p.pr, p.pb, p.pg};
+    const int order[3] = {2, 0, 1};  // surfactant, red, blue
+    for (int plane = 0; plane < 2; ++plane) {
+      const int z = plane == 0 ? 1 : nz;
+      for (int y = 1; y <= ny; ++y)
+        for (int x = 1; x <= nx; ++x) {
+          Site &s = at(x, y, z);
+          if (s.rock != 0.0) continue;
+          for (int k = 0; k < 3; ++k) {
+            const int c = order[k];
+            if (c >= nc) continue;
+            double F[19];
+            for (int q = 0; q < 19; ++q) F[q] = s.n[c][q] * (double)G[q];
+            zouhe_flux_site(F, uzc[c], plane == 0, p.inv_type);
+            for (int q = 0; q < 19; ++q) s.n[c][q] = F[q] / (double)G[q];
+            if (c == 2) {
+              for (int a = 0; a < 3; ++a) s.da[a] = 0.0;
+              for (int q = 0; q < 19; ++q) {
+                const Site &b = at(x - CX[q], y - CY[q], z - CZ[q]);
+                for (int a = 0; a < 3; ++a) s.da[a] = s.da[a] + s.n[2][q] * (double)G[q] * b.db[a];
+              }
+            }
+          }
+        }
+    }
+  }
+
   void bc_apply(int stage) {
     if (stage == 6) {
       if (le) {
@@ -572,6 +668,8 @@ struct Oracle {
         halo_periodic();
       }
     } else if (stage == 8) {
+      // code/lb3d_bc.F90:125-133: invasion first, then the halo exchange
+      if (p.boundary_cond != 0 && p.inv_fluid == 12) invade_zouhe_flux();
       exchange();
     }
   }
@@ -607,9 +705,9 @@ void *lb3do_create(const lb3do_params *p) {
   bool le = (p->boundary_cond != 0) && (p->inv_fluid == 5 || p->inv_fluid == 6);
   // code/lb3d_compatibility.F90:105-111: ternary + Lees-Edwards is fatal.
   if (p->ncomp == 3 && le) return nullptr;
-  // Invasion boundaries other than the Lees-Edwards no-ops are outside
-  // this restatement (code/lb3d_bc.F90:129-133).
-  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le) return nullptr;
+  // Invasion boundaries other than the Lees-Edwards no-ops and the Zou-He
+  // flux boundaries are outside this restatement (code/lb3d_bc.F90:129-133).
+  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && p->inv_fluid != 12) return nullptr;
   Oracle *o = new Oracle();
   o->p = *p;
   o->nx = p->nx;

@@ -39,6 +39,8 @@ typedef struct lb3do_params {
   double rock_colour_r, rock_colour_b;
   int bdist;
   int restore; /* 1: state came from a checkpoint (init_cond = 7) */
+  int inv_type; /* Zou-He closure (inv_fluid = 12) */
+  double pr, pg, pb;
 } lb3do_params;
 
 /* Returns NULL on an unsupported parameter combination. */

@@ -11,12 +11,13 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 # Compile-time mixture of each reference test (test/<T>/<T>.cfg FLAGS):
 # -DNOSURFACTANT builds are binary.
-CASES = {"gyroid": 3, "bodyForce": 3, "leesEdwards": 2, "wettingWall": 2}
+CASES = {"gyroid": 3, "bodyForce": 3, "leesEdwards": 2, "wettingWall": 2, "zouHe": 3}
 FIELDS = {
     "gyroid": ["od", "wd", "sur", "dir", "vel", "arr"],
     "bodyForce": ["od", "wd", "sur", "dir", "vel", "arr"],
     "leesEdwards": ["od", "wd", "vel", "arr"],
     "wettingWall": ["od", "wd", "vel", "arr", "rock"],
+    "zouHe": ["od", "wd", "sur", "dir", "vel", "arr"],
 }
 STAMP = "t00000000-0000000000"
 

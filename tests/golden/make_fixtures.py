@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures under tests/golden/ from the reference's
 own integration tests (testLB3D.sh, test/<T>/).
 
-For each test T in gyroid, bodyForce, leesEdwards, wettingWall the reference
+For each test T in gyroid, bodyForce, leesEdwards, wettingWall, zouHe the reference
 ships a t=0 checkpoint (checkpoint_*, checktopo_*, checkparams_* XDR files),
 the input file T.in with its dump_xdr.din override, an obstacle file where
 the test uses one, and the FP32 XDR dumps at t=10 (reference/*-t00000010.xdr)
@@ -16,7 +16,7 @@ import os
 import shutil
 import sys
 
-TESTS = ["gyroid", "bodyForce", "leesEdwards", "wettingWall"]
+TESTS = ["gyroid", "bodyForce", "leesEdwards", "wettingWall", "zouHe"]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

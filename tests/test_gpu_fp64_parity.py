@@ -250,3 +250,35 @@ def test_sanity_velocity_ties_and_fast_sites():
     np.testing.assert_array_equal(a["maxvel"], b["maxvel"])
     np.testing.assert_array_equal(a["maxpos"], b["maxpos"])
     assert a["n_too_fast"] == b["n_too_fast"] == 2
+
+
+@pytest.mark.parametrize("nc,itype", [(2, 0), (2, 1), (3, -1), (3, 0), (3, 1)])
+def test_zouhe_flux_boundaries(nc, itype):
+    """Zou-He flux boundaries on the z planes (inv_fluid 12) for every
+    closure, binary with rock sites on the boundary planes and ternary,
+    bit-identical to the oracle."""
+    dims = (10, 7, 9)
+    p = _params(dims, nc, boundary_cond=-1, inv_fluid=12, inv_type=itype, pr=0.01, pb=-0.004,
+                pg=0.002)
+    st = uniform_mixture(*dims, nc, seed=11)
+    if nc == 2:
+        rock = np.zeros((9, 7, 10))
+        rock[0, 2, 3:6] = 1.0
+        rock[8, 5, 1] = 1.0
+        rock[4, :, 7] = 1.0
+        st["rock"] = rock
+    lat = _lattice(p, st)
+    o = Oracle(p, st)
+    for _ in range(3):
+        lat.time_loop(5)
+        o.run(5)
+        assert_state_equal(lat, o, f"zouHe nc={nc} itype={itype}")
+
+
+def test_zouhe_limits():
+    from lb3d_b200.lib import Lattice, Lb3dError
+    p = _params((8, 8, 8), 2, boundary_cond=-1, inv_fluid=12)
+    with pytest.raises(Lb3dError):
+        Lattice(p, precision=1)  # FP32 path: refused
+    with pytest.raises(Lb3dError):
+        Lattice(_params((8, 8, 1), 2, boundary_cond=-1, inv_fluid=12), precision=0)
