@@ -47,7 +47,7 @@ struct lb3dc_ensemble {
   int max_lat = 0, tile_cap = 0, ntiles = 0, grid = 0;
   std::vector<Member> members;
   std::map<long long, long long> free_ranges;  // base -> length
-  FusedShape shape{16, 8, 8, 2};
+  FusedShape shape{32, 4, 8, 2};  // fastest measured on the parameter-sweep stream
   float4 *M = nullptr, *J = nullptr;
   double *stage = nullptr;  // FP64 staging of one member's populations (admit / retire)
   size_t stage_bytes = 0;

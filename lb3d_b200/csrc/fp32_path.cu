@@ -600,6 +600,25 @@ __global__ void k_from_fp64(const double *__restrict__ n, float *__restrict__ f,
     }
 }
 
+// One population plane FP64 <-> FP32 deviations (w = w_q rho0), rounded as
+// k_to_fp64 / k_from_fp64; the upload writes both buffers.
+__global__ void k_plane_from_fp64(const double *__restrict__ src, float *__restrict__ d0,
+                                  float *__restrict__ d1, long long N, double w,
+                                  const uint8_t *__restrict__ rock) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double v = (rock && rock[i] != 0) ? 0.0 : src[i];
+  const float x = (float)__dsub_rn(v, w);
+  d0[i] = x;
+  d1[i] = x;
+}
+__global__ void k_plane_to_fp64(const float *__restrict__ src, double *__restrict__ dst, long long N,
+                                double w) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  dst[i] = __dadd_rn((double)src[i], w);
+}
+
 }  // namespace f32
 
 using namespace f32;
@@ -895,7 +914,7 @@ long long fp32_footprint(const lb3dc_params &p) {
   const long long np = (long long)p.ny * p.nz;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
          N * (fp32_moment_bytes(p.ncomp) + fp32_own_bytes(p.ncomp)) +
-         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) : 0) + 4096;
+         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) : 0) + N * 8 + 4096;
 }
 
 // The Lees-Edwards halo planes of a single lattice, referenced by its descriptor.
@@ -1032,6 +1051,8 @@ int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStre
   if (cudaMalloc(&s.J, (size_t)N * fp32_own_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
   s.bytes += N * (fp32_moment_bytes(P.nc) + fp32_own_bytes(P.nc));
   if (cudaMalloc(&s.d_lat, sizeof(LatDesc)) != cudaSuccess) return LB3DC_ENOMEM;
+  if (cudaMalloc(&s.stage, (size_t)N * sizeof(double)) != cudaSuccess) return LB3DC_ENOMEM;
+  s.bytes += N * (long long)sizeof(double);
   if (P.le) {
     const size_t np = (size_t)P.ny * P.nz;
     for (int b = 0; b < 2; ++b) {
@@ -1056,6 +1077,8 @@ void fp32_free(Fp32State &s) {
   if (s.d_tiles) cudaFree(s.d_tiles);
   if (s.M) cudaFree(s.M);
   if (s.J) cudaFree(s.J);
+  if (s.stage) cudaFree(s.stage);
+  s.stage = nullptr;
   for (int b = 0; b < 2; ++b) {
     if (s.le_h[b]) cudaFree(s.le_h[b]);
     if (s.le_p[b]) cudaFree(s.le_p[b]);
@@ -1083,18 +1106,19 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   s.lat = fp32_make_desc(P, rho0, 0, any);
   attach_le(s);
   s.lat.parity = 0;
-  // FP64 staging on the device, converted to deviations by a kernel
-  double *dn = nullptr;
-  const size_t nb = (size_t)P.nc * 19 * N * sizeof(double);
-  if (cudaMalloc(&dn, nb) != cudaSuccess) return LB3DC_ENOMEM;
-  cudaError_t e = cudaMemcpyAsync(dn, n, nb, cudaMemcpyHostToDevice, st);
-  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-    k_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dn, s.f[b], s.S, 0, N, P.nc, rho0,
-                                                             any ? rockp : nullptr);
+  // one FP64 population plane at a time through the staging buffer,
+  // converted to deviations into both buffers
+  cudaError_t e = cudaSuccess;
+  for (int cq = 0; cq < P.nc * 19 && e == cudaSuccess; ++cq) {
+    const double w = (cq % 19 == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+    e = cudaMemcpyAsync(s.stage, n + (size_t)cq * N, (size_t)N * sizeof(double),
+                        cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) break;
+    k_plane_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
+        s.stage, s.f[0] + (size_t)cq * s.S, s.f[1] + (size_t)cq * s.S, N, w, any ? rockp : nullptr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(dn);
   if (e != cudaSuccess) return LB3DC_ECUDA;
   if (P.nc == 3) {
     // (ternary lattices have no rock: refused above)
@@ -1128,15 +1152,18 @@ int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, doubl
     nn = tmp.data();
   }
   if (nn) {
-    // deviations -> FP64 populations on the device, one copy back
-    double *dn = nullptr;
-    const size_t nb = (size_t)nc * 19 * N * sizeof(double);
-    if (cudaMalloc(&dn, nb) != cudaSuccess) return LB3DC_ENOMEM;
-    k_to_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.f[cur], dn, s.S, 0, N, nc, rho0);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(nn, dn, nb, cudaMemcpyDeviceToHost, st);
+    // deviations -> FP64 populations, one plane at a time through the staging buffer
+    cudaError_t e = cudaSuccess;
+    for (int cq = 0; cq < nc * 19 && e == cudaSuccess; ++cq) {
+      const double w = (cq % 19 == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+      k_plane_to_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.f[cur] + (size_t)cq * s.S,
+                                                                    s.stage, N, w);
+      e = cudaGetLastError();
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(nn + (size_t)cq * N, s.stage, (size_t)N * sizeof(double),
+                            cudaMemcpyDeviceToHost, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(dn);
     if (e != cudaSuccess) return LB3DC_ECUDA;
   }
   std::vector<uint8_t> rk(N, 0);

@@ -57,6 +57,7 @@ struct Fp32State {
   int grid = 0;
   long long bytes = 0;
   KernelTimer *timer = nullptr;  // optional, owned by the handle
+  double *stage = nullptr;  // one FP64 population plane (N sites) for uploads and downloads
   float *le_h[2] = {nullptr, nullptr};  // Lees-Edwards halo planes (see LatDesc)
   float2 *le_p[2] = {nullptr, nullptr};
 };

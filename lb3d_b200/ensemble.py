@@ -64,7 +64,7 @@ def member_bytes(p: Params) -> int:
 
 
 class Ensemble:
-    def __init__(self, ncomp=3, capacity_sites=1 << 24, max_lattices=1024, shape=(16, 8, 8, 2)):
+    def __init__(self, ncomp=3, capacity_sites=1 << 24, max_lattices=1024, shape=(32, 4, 8, 2)):
         L = _bind()
         h = ctypes.c_void_p()
         rc = L.lb3dc_ensemble_create(int(ncomp), int(capacity_sites), int(max_lattices), ctypes.byref(h))
