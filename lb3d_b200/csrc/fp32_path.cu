@@ -155,6 +155,23 @@ __device__ __forceinline__ void own_moments(const float *d, float &dr, float &j0
   j1 = a1;
   j2 = a2;
 }
+// own_moments2 of values already in registers (lane x, lane y).
+__device__ __forceinline__ void own_moments2_reg(const float2 v[19], float2 &dr, float2 &j0,
+                                                 float2 &j1, float2 &j2) {
+  float2 r = f2(0.f), a0 = f2(0.f), a1 = f2(0.f), a2 = f2(0.f);
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const float g = (float)gw(q);
+    r = fma2(f2(g), v[q], r);
+    if (cx(q)) a0 = fma2(f2(g * (float)cx(q)), v[q], a0);
+    if (cy(q)) a1 = fma2(f2(g * (float)cy(q)), v[q], a1);
+    if (cz(q)) a2 = fma2(f2(g * (float)cz(q)), v[q], a2);
+  }
+  dr = r;
+  j0 = a0;
+  j1 = a1;
+  j2 = a2;
+}
 // own_moments of two components (lanes x, y) with paired instructions.
 template <int ST>
 __device__ __forceinline__ void own_moments2(const float *dA, const float *dB, float2 &dr,
@@ -488,9 +505,9 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
               // ---- ternary Shan-Chen force, code/lb3d_force_shanchen.F90:215-330
               const int itB = itC + 1;  // B computed plane zC at iteration itC + 1
               const int bs = (tx + 1) + BW * (ty + 1);
-              force_ternary<AW, BW>(Am + AN, A0 + AN, Ap + AN, ringB + ((itB + 2) % 3) * BN,
-                                    ringB + (itB % 3) * BN, ringB + ((itB + 1) % 3) * BN, as, bs, Lg,
-                                    psi0, reinterpret_cast<float(*)[3]>(Fx));
+              force_ternary<AW, BW>(Am + AN, A0 + AN, Ap + AN, DipF4{ringB + ((itB + 2) % 3) * BN},
+                                    DipF4{ringB + (itB % 3) * BN}, DipF4{ringB + ((itB + 1) % 3) * BN},
+                                    as, bs, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
             } else {
               // ---- binary Shan-Chen force with walls, :127-210
               force_binary<AW, ROCK>(Am, A0, Ap, as, nb, RK, Lg, psi0,
@@ -646,7 +663,7 @@ size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
   const size_t AN1 = (size_t)(sh.tx + 2) * (sh.ty + 2);
   if (mode == MODE_DIPOLE) return 16 * 5 * AN1 + (size_t)4 * 5 * sh.tx * sh.ty;
   if (mode == MODE_COLLIDE2)  // Collide2Geom: ring slots x entry bytes + population stage
-    return 5 * AN1 * (nc == 3 ? 32 : 8) + (size_t)19 * nc * sh.tx * sh.ty * 4;
+    return 5 * AN1 * (nc == 3 ? 16 + 12 : 8) + (size_t)19 * nc * sh.tx * sh.ty * 4;
   if (mode == MODE_COLLIDE) return 16 * 3 * AN1 * (nc == 3 ? 2 : 1);
   const int H = mode == MODE_MOMENTS ? 0 : (nc == 3 ? 2 : 1);
   const int dh = mode == MODE_MOMENTS ? 1 : 3;

@@ -157,8 +157,9 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
             const float4 *Pm = ringP + ((it - 2) % 3) * AN, *P0 = ringP + ((it - 1) % 3) * AN;
             float Fx[NC][3];
             if (NC == 3)
-              force_ternary<AW, AW>(Pm, P0, slotP, ringB + ((it - 2) % 3) * AN, ringB + ((it - 1) % 3) * AN,
-                                slotB, as, as, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
+              force_ternary<AW, AW>(Pm, P0, slotP, DipF4{ringB + ((it - 2) % 3) * AN},
+                                    DipF4{ringB + ((it - 1) % 3) * AN}, DipF4{slotB}, as, as, Lg, psi0,
+                                    reinterpret_cast<float(*)[3]>(Fx));
             else
               force_binary<AW, ROCK>(Pm, P0, slotP, as, nb, RK, Lg, psi0,
                                      reinterpret_cast<float(*)[3]>(Fx));
@@ -248,7 +249,8 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
 // bit for bit.
 // ---------------------------------------------------------------------------
 // Shared-memory layout of k_split_collide2 (bytes): psi ring [5][AN] float4
-// (float2 for binary), dipole ring [5][AN] float4 (ternary), population
+// (float2 for binary), dipole ring [5][3][AN] float (ternary; one plane per
+// axis, so the 4-byte copies into it do not collide in banks), population
 // stage [19*NC][NT] float.
 // Five ring slots (one barrier per plane).  Three CTAs of 128 threads per
 // SM (at most 168 registers) measured faster than four CTAs at 128 registers
@@ -259,7 +261,7 @@ struct Collide2Geom {
   static constexpr int RS = 5, MINB = NT >= 256 ? 2 : 3;
   static constexpr int PB = (NC == 3) ? 16 : 8;  // psi entry bytes
   static constexpr int P_BYTES = RS * AN * PB;
-  static constexpr int B_BYTES = (NC == 3) ? RS * AN * 16 : 0;
+  static constexpr int B_BYTES = (NC == 3) ? RS * AN * 12 : 0;
   static constexpr int F_BYTES = 19 * NC * NT * 4;
   static constexpr int SMEM = P_BYTES + B_BYTES + F_BYTES;
 };
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
   extern __shared__ __align__(16) unsigned char smraw[];
   float4 *ringP4 = reinterpret_cast<float4 *>(smraw);          // ternary psi ring
   float2 *ringP2 = reinterpret_cast<float2 *>(smraw);          // binary psi ring
-  float4 *ringB = reinterpret_cast<float4 *>(smraw + G::P_BYTES);
+  float *ringB = reinterpret_cast<float *>(smraw + G::P_BYTES);  // [RS][3][AN]
   float *stage = reinterpret_cast<float *>(smraw + G::P_BYTES + G::B_BYTES);
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   float *mystage = stage + tid;
@@ -341,11 +343,11 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
         const int iy = small ? pmod(vy, ny) : wrap_small(vy, ny);
         const int i = ix + nx * (iy + ny * gz);
         if (NC == 3) {
-          cp_async16(ringP4 + sl + s, Mb + S + i);  // {da_z, dpsi_r, dpsi_b, dpsi_s}
-          float *b = reinterpret_cast<float *>(ringB + sl + s);
+          cp_async16(ringP4 + sl + s, Mb + S + i);  // {drho_s, dpsi_r, dpsi_b, dpsi_s}
+          float *b = ringB + 3 * sl + s;
           cp_async4(b, DBn + i);
-          cp_async4(b + 1, DBn + S + i);
-          cp_async4(b + 2, DBn + 2 * S + i);
+          cp_async4(b + AN, DBn + S + i);
+          cp_async4(b + 2 * AN, DBn + 2 * S + i);
         } else if (LE && vx == -1) {  // sheared halo below x = 0
           cp_async8(ringP2 + sl + s, Lg.le_p[0] + iy + ny * gz);
         } else if (LE && vx == nx) {  // sheared halo above x = nx - 1
@@ -398,9 +400,10 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
         const int as = (tx + 1) + AW * (ty + 1);
         if constexpr (NC == 3) {
           force_ternary<AW, AW>(ringP4 + (k % RS) * AN, ringP4 + ((k + 1) % RS) * AN,
-                            ringP4 + ((k + 2) % RS) * AN, ringB + (k % RS) * AN,
-                            ringB + ((k + 1) % RS) * AN, ringB + ((k + 2) % RS) * AN, as, as, Lg, psi0,
-                            reinterpret_cast<float(*)[3]>(Fx));
+                                ringP4 + ((k + 2) % RS) * AN, DipAxes{ringB + 3 * (k % RS) * AN, AN},
+                                DipAxes{ringB + 3 * ((k + 1) % RS) * AN, AN},
+                                DipAxes{ringB + 3 * ((k + 2) % RS) * AN, AN}, as, as, Lg, psi0,
+                                reinterpret_cast<float(*)[3]>(Fx));
         } else {
           // binary rings hold {dpsi_r, dpsi_b}
           const float2 *Qm = ringP2 + (k % RS) * AN, *Q0 = ringP2 + ((k + 1) % RS) * AN,
@@ -409,18 +412,28 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
         }
       }
       cp_async_wait<1>();  // this thread's pulls of plane k landed
+      bool next_skip = true;
       if (act && !skip) {
+        // the staged pulls, read once: red/blue on paired lanes, the surfactant alone
+        float2 d01[19];
+        float ds[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+          d01[q] = make_float2(mystage[q * NT], mystage[(19 + q) * NT]);
+          if (NC == 3) ds[q] = mystage[(38 + q) * NT];
+        }
+        // the stage column is free again: the next plane's pulls fly during
+        // this site's moments and BGK update
+        if (k + 1 < zc) next_skip = issue_pulls(k + 1);
         float dr[NC], rho[NC], j[NC][3];
         {
-          // components 0 and 1 on paired lanes, the surfactant alone
           float2 r2, a0, a1, a2;
-          own_moments2<NT>(mystage, mystage + 19 * NT, r2, a0, a1, a2);
+          own_moments2_reg(d01, r2, a0, a1, a2);
           dr[0] = r2.x, dr[1] = r2.y;
           j[0][0] = a0.x, j[1][0] = a0.y;
           j[0][1] = a1.x, j[1][1] = a1.y;
           j[0][2] = a2.x, j[1][2] = a2.y;
-          if (NC == 3)
-            own_moments<NT>(mystage + 2 * 19 * NT, dr[NC - 1], j[NC - 1][0], j[NC - 1][1], j[NC - 1][2]);
+          if (NC == 3) own_moments<1>(ds, dr[NC - 1], j[NC - 1][0], j[NC - 1][1], j[NC - 1][2]);
 #pragma unroll
           for (int c = 0; c < NC; ++c) rho[c] = rho0 + dr[c];
         }
@@ -464,32 +477,26 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
           vz[c] = fmaf(kf, Fx[c][2], u2);
         }
         {
-          float2 d[19];
-#pragma unroll
-          for (int q = 0; q < 19; ++q) d[q] = make_float2(mystage[q * NT], mystage[(19 + q) * NT]);
-          bgk_update2(d, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+          bgk_update2(d01, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
                       make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
                       make_float2(Lg.omega[0], Lg.omega[1]));
           float *fo = Fo + self;
 #pragma unroll
           for (int q = 0; q < 19; ++q) {
-            __stcs(fo + q * S, d[q].x);
-            __stcs(fo + (19 + q) * S, d[q].y);
+            __stcs(fo + q * S, d01[q].x);
+            __stcs(fo + (19 + q) * S, d01[q].y);
           }
         }
         if (NC == 3) {
-          float d[19];
-          const float *sc = mystage + 2 * 19 * NT;
-#pragma unroll
-          for (int q = 0; q < 19; ++q) d[q] = sc[q * NT];
-          bgk_update(d, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1], Lg.omega[NC - 1]);
+          bgk_update(ds, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1], Lg.omega[NC - 1]);
           float *fo = Fo + 2 * 19 * S + self;
 #pragma unroll
-          for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
+          for (int q = 0; q < 19; ++q) __stcs(fo + q * S, ds[q]);
         }
+      } else if (k + 1 < zc) {
+        next_skip = issue_pulls(k + 1);
       }
-      // the stage column is free again: start the next plane's pulls
-      skip = (k + 1 < zc) ? issue_pulls(k + 1) : true;
+      skip = next_skip;
       cp_async_commit();
     }
     cp_async_wait<0>();

@@ -45,11 +45,27 @@ __device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0
 //   f_cs = SA - 2V, f_sc = SG d - 2 T d, f_ss = M^T d + M d + tr(M) d - 2 Q d
 // with a = d(y) psi_s(y), SA = sum g a, V = sum g (a.c) c, G = g (psi_b -
 // psi_r), SG = sum G, T = sum G c c^T, M = sum 8g a c^T, Q = sum 8g (a.c) c c^T.
-template <int WP, int WB>
+// Dipole ring planes, read as float3 at an entry index: float4 entries
+// {d_x, d_y, d_z, -}, or three axis planes of `np` entries each.
+struct DipF4 {
+  const float4 *p;
+  __device__ __forceinline__ float3 operator()(int i) const {
+    const float4 v = p[i];
+    return make_float3(v.x, v.y, v.z);
+  }
+};
+struct DipAxes {
+  const float *p;
+  int np;
+  __device__ __forceinline__ float3 operator()(int i) const {
+    return make_float3(p[i], p[np + i], p[2 * np + i]);
+  }
+};
+
+template <int WP, int WB, typename DR>
 __device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0, const float4 *Pp,
-                                              const float4 *Bm, const float4 *B0, const float4 *Bp,
-                                              int ap, int bp, const LatDesc &Lg, float psi0,
-                                              float Fx[3][3]) {
+                                              DR Bm, DR B0, DR Bp, int ap, int bp,
+                                              const LatDesc &Lg, float psi0, float Fx[3][3]) {
   // paired accumulators: FB[k] = (f_rb, f_br)_k, SA01 = (SA_x, SA_y),
   // M01[k] = (M_xk, M_yk), TQ[K] = (T_K, Q_K)
   float2 FB[3] = {f2(0.f), f2(0.f), f2(0.f)}, M01[3] = {f2(0.f), f2(0.f), f2(0.f)};
@@ -59,11 +75,11 @@ __device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0
 #pragma unroll
   for (int q = 0; q < 18; ++q) {
     const float4 *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
-    const float4 *Bq = cz(q) == 1 ? Bp : (cz(q) == -1 ? Bm : B0);
+    const DR &Bq = cz(q) == 1 ? Bp : (cz(q) == -1 ? Bm : B0);
     const float g = (float)gw(q);
     const int c[3] = {cx(q), cy(q), cz(q)};
     const float4 e = Pq[ap + cx(q) + WP * cy(q)];
-    const float4 b = Bq[bp + cx(q) + WB * cy(q)];
+    const float3 b = Bq(bp + cx(q) + WB * cy(q));
     const float ps = psi0 + e.w;
     const float2 a01 = mul2(make_float2(b.x, b.y), f2(ps));
     const float a2 = b.z * ps;
@@ -100,7 +116,7 @@ __device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0
   const float Q[6] = {TQ[0].y, TQ[1].y, TQ[2].y, TQ[3].y, TQ[4].y, TQ[5].y};
   const float M[3][3] = {{M01[0].x, M01[1].x, M01[2].x}, {M01[0].y, M01[1].y, M01[2].y},
                          {M2[0], M2[1], M2[2]}};
-  const float4 dd = B0[bp];
+  const float3 dd = B0(bp);
   const float d[3] = {dd.x, dd.y, dd.z};
   const float4 own = P0[ap];
   const float psr = psi0 + own.y, psb = psi0 + own.z, pss = psi0 + own.w;
