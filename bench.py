@@ -37,8 +37,10 @@ L = 128
 BYTES_PER_SITE = {("f32", 3): 480, ("f32", 2): 304, ("f64", 3): 960, ("f64", 2): 608}
 # DRAM bytes per site and step that ncu measured (dram__bytes_read.sum +
 # dram__bytes_write.sum of the moments, dipole and staged collide passes) on
-# the ternary 128^3 workload with 32x4 tiles, 8-plane chunks, strategy 2.
-NCU_TRAFFIC_PER_SITE = {(32, 4, 8, 2): 774}
+# the ternary 128^3 workload, keyed by (tile x, tile y, strategy); captured
+# with 8-plane chunks (the chunk depth moves only the ring halo reloads,
+# under 1 % of this figure).
+NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 774}
 PHYS = dict(tau_d=1.0, g_br=0.08, g_bs=-0.006, g_ss=-0.0045, beta=10.0, d_0=1.0, bdist=2, restore=1)
 
 
@@ -415,8 +417,8 @@ def main():
                        "shape_source": "fixed" if args.shape else "autotuned"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
-                         "traffic": (NCU_TRAFFIC_PER_SITE[tuple(shape)] * N
-                                     if tuple(shape) in NCU_TRAFFIC_PER_SITE else None),
+                         "traffic": (NCU_TRAFFIC_PER_SITE[(shape[0], shape[1], shape[3])] * N
+                                     if (shape[0], shape[1], shape[3]) in NCU_TRAFFIC_PER_SITE else None),
                          "traffic_note": "DRAM bytes per step from one ncu capture of the three passes "
                                          "(null for launch shapes without a capture)",
                          "peak_kind": peak_kind,
