@@ -261,6 +261,18 @@ int lb3dc_ensemble_finished(lb3dc_ensemble *e, int *slots, int max, int *count);
 /* Downloads a member's populations/dipoles (either may be NULL) and frees
  * its slot and site range (synchronising). */
 int lb3dc_ensemble_retire(lb3dc_ensemble *e, int slot, double *n, double *db);
+/* Asynchronous retire of a finished member: its FP64 populations (and
+ * dipoles) are converted and copied to n (db) on a copy stream while the
+ * other members keep stepping; n and db should be pinned host memory
+ * (lb3dc_host_alloc) for the copies to overlap.  The slot and its site
+ * range stay reserved until lb3dc_ensemble_poll reports the copies done. */
+int lb3dc_ensemble_retire_async(lb3dc_ensemble *e, int slot, double *n, double *db);
+/* *done = 1 (and the slot freed) once the asynchronous retire of slot has
+ * landed on the host, else *done = 0. */
+int lb3dc_ensemble_poll(lb3dc_ensemble *e, int slot, int *done);
+/* Page-locked host memory for asynchronous copies. */
+int lb3dc_host_alloc(long long bytes, void **ptr);
+int lb3dc_host_free(void *ptr);
 int lb3dc_ensemble_stats(const lb3dc_ensemble *e, long long *free_sites, int *active,
                          int *resident, long long *site_updates);
 long long lb3dc_ensemble_bytes(const lb3dc_ensemble *e);

@@ -30,6 +30,8 @@ struct Member {
   int remaining = 0;   // steps still to run
   int done_steps = 0;
   bool finished = false;
+  bool retiring = false;             // results on their way to the host (async retire)
+  cudaEvent_t copied = nullptr;      // recorded on the copy stream after the last copy
   LatDesc desc{};
   lb3dc_params p{};
 };
@@ -51,6 +53,9 @@ struct lb3dc_ensemble {
   float4 *M = nullptr, *J = nullptr;
   double *stage = nullptr;  // FP64 staging of one member's populations (admit / retire)
   size_t stage_bytes = 0;
+  cudaStream_t copy_stream = nullptr;  // asynchronous retires
+  double *cstage = nullptr;            // their FP64 staging (populations, then dipoles)
+  size_t cstage_bytes = 0;
   bool dirty = true;  // tile list must be rebuilt
   bool body = false;
   cudaGraph_t graph = nullptr;
@@ -312,6 +317,13 @@ int lb3dc_ensemble_destroy(lb3dc_ensemble *e) {
   if (e->d_lat) cudaFree(e->d_lat);
   if (e->d_tiles) cudaFree(e->d_tiles);
   if (e->stage) cudaFree(e->stage);
+  if (e->copy_stream) {
+    cudaStreamSynchronize(e->copy_stream);
+    cudaStreamDestroy(e->copy_stream);
+  }
+  for (auto &m : e->members)
+    if (m.copied) cudaEventDestroy(m.copied);
+  if (e->cstage) cudaFree(e->cstage);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return LB3DC_OK;
@@ -461,6 +473,7 @@ int lb3dc_ensemble_retire(lb3dc_ensemble *e, int slot, double *n, double *db) {
     return efail(e, LB3DC_EINVAL, "bad slot");
   cudaSetDevice(e->device);
   Member &m = e->members[slot];
+  if (m.retiring) return efail(e, LB3DC_ESTATE, "member is being retired asynchronously");
   const long long N = m.n;
   const int cur = m.desc.parity;
   cudaStreamSynchronize(e->stream);
@@ -487,8 +500,89 @@ int lb3dc_ensemble_retire(lb3dc_ensemble *e, int slot, double *n, double *db) {
   cudaMemcpyAsync(e->d_lat + slot, &off, sizeof(LatDesc), cudaMemcpyHostToDevice, e->stream);
   cudaStreamSynchronize(e->stream);
   give_range(e, m.base, m.n);
+  cudaEvent_t keep = m.copied;
   m = Member();
+  m.copied = keep;
   e->dirty = true;
+  return LB3DC_OK;
+}
+
+int lb3dc_ensemble_retire_async(lb3dc_ensemble *e, int slot, double *n, double *db) {
+  if (!e || slot < 0 || slot >= e->max_lat || !e->members[slot].used)
+    return efail(e, LB3DC_EINVAL, "bad slot");
+  Member &m = e->members[slot];
+  if (!m.finished || m.retiring) return efail(e, LB3DC_ESTATE, "member is not finished");
+  cudaSetDevice(e->device);
+  if (!e->copy_stream && cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return efail(e, LB3DC_ECUDA, "copy stream creation failed");
+  const long long N = m.n;
+  const int cur = m.desc.parity;
+  const size_t nb = (size_t)e->nc * 19 * N * sizeof(double), dbb = 3 * (size_t)N * sizeof(double);
+  if (e->cstage_bytes < nb + dbb) {
+    // the staging is reused in stream order; grow it only when no copy is in flight
+    cudaStreamSynchronize(e->copy_stream);
+    if (e->cstage) cudaFree(e->cstage);
+    e->cstage = nullptr;
+    e->cstage_bytes = 0;
+    if (cudaMalloc(&e->cstage, nb + dbb) != cudaSuccess) return efail(e, LB3DC_ENOMEM, "staging allocation failed");
+    e->cstage_bytes = nb + dbb;
+  }
+  // the member's last step is queued on the main stream before this point;
+  // later steps do not touch it (it is no longer active)
+  cudaEvent_t after;
+  if (cudaEventCreateWithFlags(&after, cudaEventDisableTiming) != cudaSuccess)
+    return efail(e, LB3DC_ECUDA, "event creation failed");
+  cudaEventRecord(after, e->stream);
+  cudaStreamWaitEvent(e->copy_stream, after, 0);
+  cudaEventDestroy(after);
+  cudaError_t r = cudaSuccess;
+  if (n) {
+    r = fp32_to_fp64(e->f[cur], e->cstage, e->S, m.base, N, e->nc, m.desc.rho0, e->copy_stream);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(n, e->cstage, nb, cudaMemcpyDeviceToHost, e->copy_stream);
+  }
+  if (r == cudaSuccess && db && e->nc == 3) {
+    double *dst = e->cstage + (size_t)e->nc * 19 * N;
+    r = fp32_planes_to_fp64(e->db[cur], dst, e->S, m.base, N, 3, e->copy_stream);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(db, dst, dbb, cudaMemcpyDeviceToHost, e->copy_stream);
+  }
+  if (r == cudaSuccess && !m.copied) r = cudaEventCreateWithFlags(&m.copied, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventRecord(m.copied, e->copy_stream);
+  if (r != cudaSuccess) return efail(e, LB3DC_ECUDA, std::string("asynchronous retire: ") + cudaGetErrorString(r));
+  m.finished = false;
+  m.retiring = true;
+  return LB3DC_OK;
+}
+
+int lb3dc_ensemble_poll(lb3dc_ensemble *e, int slot, int *done) {
+  if (!e || !done || slot < 0 || slot >= e->max_lat || !e->members[slot].used ||
+      !e->members[slot].retiring)
+    return efail(e, LB3DC_EINVAL, "bad slot");
+  Member &m = e->members[slot];
+  *done = 0;
+  cudaError_t q = cudaEventQuery(m.copied);
+  if (q == cudaErrorNotReady) return LB3DC_OK;
+  if (q != cudaSuccess) return efail(e, LB3DC_ECUDA, std::string("asynchronous retire: ") + cudaGetErrorString(q));
+  // the copies have landed: free the slot and its range
+  cudaSetDevice(e->device);
+  LatDesc off{};
+  cudaMemcpyAsync(e->d_lat + slot, &off, sizeof(LatDesc), cudaMemcpyHostToDevice, e->stream);
+  give_range(e, m.base, m.n);
+  cudaEvent_t keep = m.copied;
+  m = Member();
+  m.copied = keep;  // reused by the slot's next retire
+  e->dirty = true;
+  *done = 1;
+  return LB3DC_OK;
+}
+
+int lb3dc_host_alloc(long long bytes, void **ptr) {
+  if (!ptr || bytes <= 0) return LB3DC_EINVAL;
+  *ptr = nullptr;
+  return cudaMallocHost(ptr, (size_t)bytes) == cudaSuccess ? LB3DC_OK : LB3DC_ENOMEM;
+}
+
+int lb3dc_host_free(void *ptr) {
+  if (ptr) cudaFreeHost(ptr);
   return LB3DC_OK;
 }
 

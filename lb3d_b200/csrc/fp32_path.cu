@@ -647,6 +647,20 @@ cudaError_t fp32_to_fp64(const float *f, double *out, long long S, long long bas
   return cudaGetLastError();
 }
 
+__global__ void k_planes_f2d(const float *__restrict__ src, double *__restrict__ dst, long long S,
+                             long long base, long long N, int planes) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int k = 0; k < planes; ++k) dst[(long long)k * N + i] = (double)src[(long long)k * S + base + i];
+}
+
+cudaError_t fp32_planes_to_fp64(const float *src, double *dst, long long S, long long base,
+                                long long N, int planes, cudaStream_t st) {
+  if (N <= 0) return cudaSuccess;
+  k_planes_f2d<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(src, dst, S, base, N, planes);
+  return cudaGetLastError();
+}
+
 cudaError_t fp32_from_fp64(const double *n, float *f, long long S, long long base, long long N,
                            int nc, double rho0, const uint8_t *rock, cudaStream_t st) {
   if (N <= 0) return cudaSuccess;

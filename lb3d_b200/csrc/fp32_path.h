@@ -117,6 +117,9 @@ cudaError_t fp32_to_fp64(const float *f, double *out, long long S, long long bas
                          int nc, double rho0, cudaStream_t st);
 cudaError_t fp32_from_fp64(const double *n, float *f, long long S, long long base, long long N,
                            int nc, double rho0, const uint8_t *rock, cudaStream_t st);
+// `planes` FP32 planes of stride S (lattice at base) widened to FP64 [planes][N].
+cudaError_t fp32_planes_to_fp64(const float *src, double *dst, long long S, long long base,
+                                long long N, int planes, cudaStream_t st);
 // Bytes per site of the split strategy's moment fields.
 inline long long fp32_moment_bytes(int nc) { return nc == 3 ? 32 : 8; }
 inline long long fp32_own_bytes(int nc) { return nc == 3 ? 48 : 32; }

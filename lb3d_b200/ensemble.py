@@ -48,6 +48,10 @@ def _bind():
         "lb3dc_ensemble_stats": (I, [V, ctypes.POINTER(LL), ctypes.POINTER(I), ctypes.POINTER(I),
                                      ctypes.POINTER(LL)]),
         "lb3dc_ensemble_bytes": (LL, [V]),
+        "lb3dc_ensemble_retire_async": (I, [V, I, _D, _D]),
+        "lb3dc_ensemble_poll": (I, [V, I, ctypes.POINTER(I)]),
+        "lb3dc_host_alloc": (I, [LL, ctypes.POINTER(V)]),
+        "lb3dc_host_free": (I, [V]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -63,6 +67,40 @@ def member_bytes(p: Params) -> int:
     return n * (2 * 19 * p.ncomp * 4 + (24 if p.ncomp == 3 else 0) + 1)
 
 
+class PinnedPool:
+    """Reusable page-locked host blocks (lb3dc_host_alloc) viewed as float64
+    arrays; a block is taken for a shape and given back after use."""
+
+    def __init__(self):
+        self.free = []    # (capacity in elements, pointer)
+        self.owned = {}   # id(array) -> (capacity, pointer)
+
+    def take(self, shape):
+        count = int(np.prod(shape))
+        for k, (cap, p) in enumerate(self.free):
+            if cap >= count:
+                self.free.pop(k)
+                break
+        else:
+            p = ctypes.c_void_p()
+            rc = _bind().lb3dc_host_alloc(ctypes.c_longlong(count * 8), ctypes.byref(p))
+            if rc != 0:
+                raise Lb3dError(rc, "pinned host allocation failed")
+            cap, p = count, p.value
+        buf = (ctypes.c_double * cap).from_address(p)
+        arr = np.ctypeslib.as_array(buf)[:count].reshape(shape)
+        self.owned[id(arr)] = (cap, p)
+        return arr
+
+    def give(self, arr):
+        self.free.append(self.owned.pop(id(arr)))
+
+    def release(self):
+        for cap, p in self.free + list(self.owned.values()):
+            _bind().lb3dc_host_free(ctypes.c_void_p(p))
+        self.free, self.owned = [], {}
+
+
 class Ensemble:
     def __init__(self, ncomp=3, capacity_sites=1 << 24, max_lattices=1024, shape=(32, 4, 8, 2)):
         L = _bind()
@@ -75,6 +113,8 @@ class Ensemble:
         self.h = h
         self.ncomp = ncomp
         self.capacity = capacity_sites
+        self._pinned = PinnedPool()
+        self._pending = {}
         if shape:
             sh = tuple(shape) + ((1,) if len(shape) == 3 else ())
             self._ck(L.lb3dc_ensemble_set_shape(self.h, *map(int, sh)))
@@ -92,6 +132,8 @@ class Ensemble:
         if getattr(self, "h", None):
             _bind().lb3dc_ensemble_destroy(self.h)
             self.h = None
+        if getattr(self, "_pinned", None):
+            self._pinned.release()
 
     def __del__(self):
         try:
@@ -147,6 +189,30 @@ class Ensemble:
             self._ck(_bind().lb3dc_ensemble_retire(self.h, int(slot), None, None))
         return out
 
+    # -- asynchronous retire --------------------------------------------
+    def retire_async(self, slot, shape):
+        """Starts copying a finished member's populations (and dipoles) to
+        pinned host buffers while the ensemble keeps stepping; `poll` tells
+        when they have landed and `collect` returns them."""
+        n = self._pinned.take((self.ncomp, 19) + tuple(shape))
+        db = self._pinned.take((3,) + tuple(shape)) if self.ncomp == 3 else None
+        self._ck(_bind().lb3dc_ensemble_retire_async(self.h, int(slot), ptr(n), ptr(db)))
+        self._pending[slot] = (n, db)
+
+    def poll(self, slot) -> bool:
+        done = ctypes.c_int()
+        self._ck(_bind().lb3dc_ensemble_poll(self.h, int(slot), ctypes.byref(done)))
+        return bool(done.value)
+
+    def collect(self, slot):
+        """Copies a landed asynchronous retire out of the pinned buffers."""
+        n, db = self._pending.pop(slot)
+        out = dict(n=n.copy(), db=None if db is None else db.copy())
+        self._pinned.give(n)
+        if db is not None:
+            self._pinned.give(db)
+        return out
+
     def stats(self):
         fs, a, r, su = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
         _bind().lb3dc_ensemble_stats(self.h, ctypes.byref(fs), ctypes.byref(a), ctypes.byref(r), ctypes.byref(su))
@@ -189,17 +255,32 @@ def sweep_requests(n, seed=7, rate=200.0, lmin=16, lmax=96, steps=(500, 5000), n
 
 
 class Server:
-    """Continuous-batching request loop over one Ensemble."""
+    """Continuous-batching request loop over one Ensemble.  Finished members
+    are retired asynchronously: their results travel to the host while the
+    others step, and a request is done when its results have landed."""
 
     def __init__(self, ensemble: Ensemble, chunk=64, download=True):
         self.ens = ensemble
         self.chunk = chunk
         self.download = download
 
+    def _collect(self, copying, done, clock, wait=False):
+        while copying:
+            landed = [s for s in list(copying) if self.ens.poll(s)]
+            for s in landed:
+                r = copying.pop(s)
+                r.result = self.ens.collect(s)
+                r.done = clock()
+                done.append(r)
+            if not wait or not copying:
+                return
+            time.sleep(0.0005)
+
     def run(self, requests: List[Request], realtime=True, time_scale=1.0):
         reqs = sorted(requests, key=lambda r: r.arrival)
         queue: List[Request] = []
         live: Dict[int, Request] = {}
+        copying: Dict[int, Request] = {}  # finished, results on their way to the host
         nxt = 0
         t0 = time.perf_counter()
         clock = lambda: (time.perf_counter() - t0) / time_scale  # noqa: E731
@@ -219,17 +300,27 @@ class Server:
                 live[slot] = r
                 queue.pop(0)
             if not live:
-                if nxt < len(reqs) and realtime:
+                if copying:
+                    self._collect(copying, done, clock, wait=True)
+                elif nxt < len(reqs) and realtime:
                     time.sleep(max(0.0, (reqs[nxt].arrival - clock()) * time_scale))
                 continue
             self.ens.step(self.chunk)
+            # while the GPU steps: hand over the results that have landed
+            self._collect(copying, done, clock)
             self.ens.sync()
             for slot in self.ens.finished():
                 r = live.pop(slot)
-                shape = (r.params.nz, r.params.ny, r.params.nx)
-                r.result = self.ens.retire(slot, shape, download=self.download)
-                r.done = clock()
-                done.append(r)
+                if self.download:
+                    self.ens.retire_async(slot, (r.params.nz, r.params.ny, r.params.nx))
+                    copying[slot] = r
+                else:
+                    self.ens.retire(slot, download=False)
+                    r.done = clock()
+                    done.append(r)
+            if not live and copying and not queue:
+                self._collect(copying, done, clock, wait=True)
+        self._collect(copying, done, clock, wait=True)
         wall = clock()
         lat = np.array([r.done - r.arrival for r in done])
         first = min(r.arrival for r in reqs)

@@ -102,3 +102,29 @@ def test_server_continuous_batching_results_match_alone():
         e1.step(1000)
     alone = e1.retire(s, (r.params.nz, r.params.ny, r.params.nx))
     np.testing.assert_array_equal(r.result["n"], alone["n"])
+
+
+def test_async_retire_equals_sync_retire_while_others_step():
+    """Two identical members: one retired synchronously, the other
+    asynchronously while a third member keeps stepping; the landed results
+    are identical and the slot frees only after poll reports the copy."""
+    from lb3d_b200.ensemble import Ensemble
+    p = _p((20, 18, 16))
+    st = uniform_mixture(20, 18, 16, 3, seed=21)
+    e = Ensemble(3, capacity_sites=100000, max_lattices=8, shape=SHAPE)
+    a = e.admit(p, st, steps=12)
+    b = e.admit(p, st, steps=12)
+    c = e.admit(_p((24, 20, 18)), uniform_mixture(24, 20, 18, 3, seed=22), steps=60)
+    while a not in e.finished():
+        e.step(100)
+    e.sync()
+    got_sync = e.retire(a, (16, 18, 20))
+    e.retire_async(b, (16, 18, 20))
+    e.step(100)  # the third member keeps going meanwhile
+    while not e.poll(b):
+        pass
+    got_async = e.collect(b)
+    np.testing.assert_array_equal(got_async["n"], got_sync["n"])
+    np.testing.assert_array_equal(got_async["db"], got_sync["db"])
+    assert e.stats()["resident"] == 1
+    e.close()

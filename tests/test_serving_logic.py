@@ -56,6 +56,23 @@ class FakeEnsemble:
         self.free = merged
         return {"slot": slot}
 
+    # asynchronous retire: the copy lands after one poll; until then the
+    # slot's range stays reserved
+    def retire_async(self, slot, shape):
+        self.members[slot][2] = -1  # no longer listed as finished
+        self.copying = getattr(self, "copying", {})
+        self.copying[slot] = 1
+
+    def poll(self, slot):
+        if self.copying[slot] > 0:
+            self.copying[slot] -= 1
+            return False
+        return True
+
+    def collect(self, slot):
+        del self.copying[slot]
+        return self.retire(slot)
+
 
 def test_sweep_requests_deterministic_and_in_range():
     a = sweep_requests(200, seed=5)
@@ -76,3 +93,16 @@ def test_server_admits_in_order_and_completes_all():
     assert fake.admit_order == [r.seed for r in sorted(reqs, key=lambda r: r.arrival)]
     assert all(r.done >= r.admitted for r in reqs)
     assert fake.free == [(0, 3 * 40 ** 3)]
+
+
+def test_server_asynchronous_retire_frees_ranges_only_after_landing():
+    """With downloads the finished members are retired asynchronously; their
+    ranges are reused only after the copies land, every request completes
+    and the whole capacity is free at the end."""
+    reqs = sweep_requests(30, seed=4, rate=1e6, lmin=16, lmax=32, steps=(10, 40))
+    fake = FakeEnsemble(capacity=2 * 32 ** 3)
+    out = Server(fake, chunk=8, download=True).run(reqs, realtime=False)
+    assert out["solves"] == 30
+    assert all(r.result is not None and r.done >= r.admitted for r in reqs)
+    assert fake.free == [(0, 2 * 32 ** 3)]
+    assert not getattr(fake, "copying", {})
