@@ -284,7 +284,6 @@ int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
   }
   ok = ok && cudaMalloc(&e->rock, (size_t)capacity_sites) == cudaSuccess;
   ok = ok && cudaMalloc(&e->M, (size_t)capacity_sites * fp32_moment_bytes(ncomp)) == cudaSuccess;
-  ok = ok && cudaMalloc(&e->J, (size_t)capacity_sites * fp32_own_bytes(ncomp)) == cudaSuccess;
   ok = ok && cudaMalloc(&e->d_lat, (size_t)max_lattices * sizeof(LatDesc)) == cudaSuccess;
   if (!ok) {
     lb3dc_ensemble_destroy(e);
@@ -293,7 +292,7 @@ int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
   cudaMemsetAsync(e->rock, 0, (size_t)capacity_sites, e->stream);
   cudaMemsetAsync(e->d_lat, 0, (size_t)max_lattices * sizeof(LatDesc), e->stream);
   e->bytes = 2 * (long long)pop + (ncomp == 3 ? 24LL * capacity_sites : 0) + capacity_sites +
-             capacity_sites * (fp32_moment_bytes(ncomp) + fp32_own_bytes(ncomp)) +
+             capacity_sites * fp32_moment_bytes(ncomp) +
              (long long)max_lattices * sizeof(LatDesc);
   e->members.resize(max_lattices);
   e->free_ranges[0] = capacity_sites;
@@ -342,6 +341,17 @@ int lb3dc_ensemble_set_shape(lb3dc_ensemble *e, int tx, int ty, int zc, int spli
   FusedShape sh{tx, ty, zc, split};
   if (fp32_fused_ctas_per_sm(e->nc, false, false, sh) < 1 || zc < 1)
     return efail(e, LB3DC_EINVAL, "unsupported launch shape");
+  // the own-moment field is read by the plain split strategy only; it is
+  // allocated the first time that strategy is chosen
+  if (split == 1 && !e->J) {
+    cudaSetDevice(e->device);
+    if (cudaMalloc(&e->J, (size_t)e->S * fp32_own_bytes(e->nc)) != cudaSuccess) {
+      e->J = nullptr;
+      cudaGetLastError();
+      return efail(e, LB3DC_ENOMEM, "own-moment field allocation failed");
+    }
+    e->bytes += e->S * fp32_own_bytes(e->nc);
+  }
   e->shape = sh;
   e->dirty = true;
   return LB3DC_OK;

@@ -944,7 +944,7 @@ long long fp32_footprint(const lb3dc_params &p) {
   const bool le = p.boundary_cond != 0 && (p.inv_fluid == 5 || p.inv_fluid == 6);
   const long long np = (long long)p.ny * p.nz;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
-         N * (fp32_moment_bytes(p.ncomp) + fp32_own_bytes(p.ncomp)) +
+         N * fp32_moment_bytes(p.ncomp) +
          (le ? 2 * np * (p.ncomp * 19 * 4 + 8) : 0) + N * 8 + 4096;
 }
 
@@ -964,7 +964,26 @@ static FusedShape default_shape(const DevParams &P) {
   return sh;
 }
 
+// The own-moment field J is read only by the plain split strategy (split 1);
+// it is allocated the first time a lattice is switched to that strategy, so
+// the other strategies hold no memory for it.
+static int ensure_own(const DevParams &P, Fp32State &s) {
+  if (s.J) return LB3DC_OK;
+  const size_t b = (size_t)P.nsites * fp32_own_bytes(P.nc);
+  if (cudaMalloc(&s.J, b) != cudaSuccess) {
+    s.J = nullptr;
+    cudaGetLastError();
+    return LB3DC_ENOMEM;
+  }
+  s.bytes += (long long)b;
+  return LB3DC_OK;
+}
+
 static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
+  if (sh.split == 1) {
+    int rc = ensure_own(P, s);
+    if (rc) return rc;
+  }
   std::vector<Tile> tiles;
   fp32_tiles_for(s.lat, 0, sh, tiles);
   if (s.d_tiles) cudaFree(s.d_tiles);
@@ -1079,8 +1098,7 @@ int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStre
     }
   }
   if (cudaMalloc(&s.M, (size_t)N * fp32_moment_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
-  if (cudaMalloc(&s.J, (size_t)N * fp32_own_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
-  s.bytes += N * (fp32_moment_bytes(P.nc) + fp32_own_bytes(P.nc));
+  s.bytes += N * fp32_moment_bytes(P.nc);
   if (cudaMalloc(&s.d_lat, sizeof(LatDesc)) != cudaSuccess) return LB3DC_ENOMEM;
   if (cudaMalloc(&s.stage, (size_t)N * sizeof(double)) != cudaSuccess) return LB3DC_ENOMEM;
   s.bytes += N * (long long)sizeof(double);
