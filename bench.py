@@ -372,9 +372,15 @@ def main():
         pg.barrier()
     t0 = time.perf_counter()
     lat.upload(host["n"], host.get("db"), host.get("rock"))
+    t1 = time.perf_counter()
     lat.time_loop(args.steps)
+    lat.sync()
+    t2 = time.perf_counter()
     lib().lb3dc_download_state(lat.h, ptr(out_n), None, None, None, None)
-    (e2e_s,) = D.max_over_ranks([time.perf_counter() - t0], dev)
+    t3 = time.perf_counter()
+    (e2e_s,) = D.max_over_ranks([t3 - t0], dev)
+    e2e_parts = {"upload_ms": round((t1 - t0) * 1e3, 2), "steps_ms": round((t2 - t1) * 1e3, 2),
+                 "download_ms": round((t3 - t2) * 1e3, 2)}
     lat.close()
     h2d = sum(v.nbytes for v in host.values())
     d2h = out_n.nbytes
@@ -430,7 +436,8 @@ def main():
             "ensemble": serve,
             "e2e": {"value": round(world * N * args.steps / e2e_s / 1e6, 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
-                    "solve": f"upload FP64 state + {args.steps} steps + download FP64 populations"},
+                    "solve": f"upload FP64 state + {args.steps} steps + download FP64 populations",
+                    **e2e_parts},
             "gpu_launches": int(alllaunch),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

@@ -359,12 +359,16 @@ int lb3dc_upload_state(lb3dc_handle *h, const double *n, const double *db, const
   // lbe_init_rock_colour (code/lb3d_ic_rock.F90:146-189): populations and
   // dipoles of rock sites are cleared -- on the device, so the caller's
   // (possibly pinned) arrays are copied as they are.
-  std::vector<uint8_t> rk(N, 0);
   bool any = false;
-  if (rock)
+  if (rock) {
+    std::vector<uint8_t> rk(N, 0);
     for (size_t i = 0; i < N; ++i)
       if (rock[i] != 0.0) rk[i] = 1, any = true;
-  CK(h, cudaMemcpyAsync(h->rock, rk.data(), N, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->rock, rk.data(), N, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));  // rk is released at the end of this block
+  } else {
+    CK(h, cudaMemsetAsync(h->rock, 0, N, h->stream));
+  }
   h->P.any_rock = any ? 1 : 0;
   if (h->p.precision == LB3DC_FP64) {
     CK(h, cudaMemcpyAsync(h->f, n, nc * 19 * N * 8, cudaMemcpyHostToDevice, h->stream));

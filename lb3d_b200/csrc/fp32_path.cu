@@ -48,6 +48,13 @@ __device__ __forceinline__ int pmod(int v, int n) {
   int r = v % n;
   return r < 0 ? r + n : r;
 }
+// Periodic wrap without a division when v lies within one period of the
+// lattice (-n <= v < 2n), the case of every tile and halo coordinate of a
+// lattice at least as large as the halo; pmod otherwise.
+__device__ __forceinline__ int wrapz(int v, int n) {
+  if (v >= -n && v < 2 * n) return v < 0 ? v + n : (v >= n ? v - n : v);
+  return pmod(v, n);
+}
 
 // Langevin function L(x) = coth x - 1/x, accurate in FP32 for small x.
 __device__ __forceinline__ float langevin(float x) {
@@ -59,26 +66,29 @@ __device__ __forceinline__ float langevin(float x) {
   return 1.0f / t - 1.0f / x;
 }
 
-// Equilibrium deviation for one component: out_i = rho*(E_i(v) - w_i) + drho*w_i
+// Equilibrium deviation for one component: deq_i = rho*(E_i(v) - w_i) + drho*w_i
 // with E of bdist = 2 (code/lb3d_bdist.F90:301-370), then the BGK update
-// d_i <- d_i + omega (deq_i - d_i).  Every multiply-add is written out
-// (fmaf), so bgk_update2 below can repeat the same roundings lane by lane.
+// d_i <- d_i + omega (deq_i - d_i), evaluated as (1 - omega) d_i + omega deq_i
+// with omega folded into the equilibrium's coefficients.  Every multiply-add
+// is written out (fmaf), so bgk_update2 below can repeat the same roundings
+// lane by lane.
 __device__ __forceinline__ void bgk_update(float d[19], float rho, float drho, float vx, float vy,
                                            float vz, float omega) {
   const float tx = 3.0f * vx, ty = 3.0f * vy, tz = 3.0f * vz;
   const float uke = 0.5f * fmaf(tz, vz, fmaf(ty, vy, tx * vx));
   const float a = -uke;          // even part minus w
   const float b = 1.0f + a;      // odd linear coefficient
-  const float rw = rho * W1;
-  const float base = drho * W1;
+  const float orw = (omega * rho) * W1;
+  const float obase = (omega * drho) * W1;
+  const float om1 = 1.0f - omega;
 #define LB3D_PAIR32(CD, I, J)                                             \
   {                                                                       \
     const float e = (CD);                                                 \
     const float e2 = e * e;                                               \
-    const float ev = fmaf(rw, fmaf(0.5f, e2, a), base);                   \
-    const float od = (rw * e) * fmaf(e2, 1.0f / 6.0f, b);                 \
-    d[I] = fmaf(omega, (ev + od) - d[I], d[I]);                           \
-    d[J] = fmaf(omega, (ev - od) - d[J], d[J]);                           \
+    const float ev = fmaf(orw, fmaf(0.5f, e2, a), obase);                 \
+    const float od = (orw * e) * fmaf(e2, 1.0f / 6.0f, b);                \
+    d[I] = fmaf(om1, d[I], ev + od);                                      \
+    d[J] = fmaf(om1, d[J], ev - od);                                      \
   }
   LB3D_PAIR32(tx, 0, 1)
   LB3D_PAIR32(ty, 2, 3)
@@ -90,8 +100,8 @@ __device__ __forceinline__ void bgk_update(float d[19], float rho, float drho, f
   LB3D_PAIR32(ty + tz, 14, 17)
   LB3D_PAIR32(ty - tz, 15, 16)
 #undef LB3D_PAIR32
-  const float deq0 = fmaf(rho * W0, a, drho * W0);
-  d[18] = fmaf(omega, deq0 - d[18], d[18]);
+  const float oeq0 = fmaf((omega * rho) * W0, a, (omega * drho) * W0);
+  d[18] = fmaf(om1, d[18], oeq0);
 }
 
 // Paired FP32 arithmetic (sm_100 FADD2/FMUL2/FFMA2: two lanes per
@@ -110,16 +120,17 @@ __device__ __forceinline__ void bgk_update2(float2 d[19], float2 rho, float2 drh
   const float2 uke = mul2(f2(0.5f), fma2(tz, vz, fma2(ty, vy, mul2(tx, vx))));
   const float2 a = neg2(uke);
   const float2 b = add2(f2(1.0f), a);
-  const float2 rw = mul2(rho, f2(W1));
-  const float2 base = mul2(drho, f2(W1));
+  const float2 orw = mul2(mul2(omega, rho), f2(W1));
+  const float2 obase = mul2(mul2(omega, drho), f2(W1));
+  const float2 om1 = add2(f2(1.0f), neg2(omega));
 #define LB3D_PAIR2(CD, I, J)                                                  \
   {                                                                           \
     const float2 e = (CD);                                                    \
     const float2 e2 = mul2(e, e);                                             \
-    const float2 ev = fma2(rw, fma2(f2(0.5f), e2, a), base);                  \
-    const float2 od = mul2(mul2(rw, e), fma2(e2, f2(1.0f / 6.0f), b));        \
-    d[I] = fma2(omega, add2(add2(ev, od), neg2(d[I])), d[I]);                 \
-    d[J] = fma2(omega, add2(add2(ev, neg2(od)), neg2(d[J])), d[J]);           \
+    const float2 ev = fma2(orw, fma2(f2(0.5f), e2, a), obase);                \
+    const float2 od = mul2(mul2(orw, e), fma2(e2, f2(1.0f / 6.0f), b));       \
+    d[I] = fma2(om1, d[I], add2(ev, od));                                     \
+    d[J] = fma2(om1, d[J], add2(ev, neg2(od)));                               \
   }
   LB3D_PAIR2(tx, 0, 1)
   LB3D_PAIR2(ty, 2, 3)
@@ -131,8 +142,8 @@ __device__ __forceinline__ void bgk_update2(float2 d[19], float2 rho, float2 drh
   LB3D_PAIR2(add2(ty, tz), 14, 17)
   LB3D_PAIR2(add2(ty, neg2(tz)), 15, 16)
 #undef LB3D_PAIR2
-  const float2 deq0 = fma2(mul2(rho, f2(W0)), a, mul2(drho, f2(W0)));
-  d[18] = fma2(omega, add2(deq0, neg2(d[18])), d[18]);
+  const float2 oeq0 = fma2(mul2(mul2(omega, rho), f2(W0)), a, mul2(mul2(omega, drho), f2(W0)));
+  d[18] = fma2(om1, d[18], oeq0);
 }
 
 // Own-site moments of one component's post-stream deviations d[q * ST]:
@@ -289,11 +300,6 @@ __device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, int S,
 //   B  ternary: new dipoles {d_x, d_y, d_z, -} on the tile + 1 halo, 3 planes
 //   D  ternary: previous dipoles on the tile + 3 halo, 3 planes
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int wrap_small(int v, int n) {
-  // valid for -n <= v < 2n
-  return v < 0 ? v + n : (v >= n ? v - n : v);
-}
-
 #include "fp32_stencil.cuh"
 
 // Kernel modes.  FUSED: one pass per step (moments recomputed on the halo).
@@ -351,14 +357,13 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
     const int niter = zc + 2 * H;
     float4 *__restrict__ Mb = Mf ? Mf + base : nullptr;  // moment field of this lattice
     float4 *__restrict__ Jb = Jf ? Jf + base : nullptr;  // own-site moments
-    // halo coordinates stay within one period of the lattice when the
-    // lattice is at least a tile plus halo wide; otherwise use modulo
-    const bool small = (nx < TX + 3) || (ny < TY + 3);
-    auto wx = [&](int v) { return small ? pmod(v, nx) : wrap_small(v, nx); };
-    auto wy = [&](int v) { return small ? pmod(v, ny) : wrap_small(v, ny); };
+    // halo coordinates wrap with wrapz (a division only when the lattice is
+    // narrower than the halo)
+    auto wx = [&](int v) { return wrapz(v, nx); };
+    auto wy = [&](int v) { return wrapz(v, ny); };
 
     auto load_db_plane = [&](int j) {
-      const int gz = pmod(zfirst - 1 + j, nz);
+      const int gz = wrapz(zfirst - 1 + j, nz);
       float4 *dst = ringD + (j % 3) * DN;
       for (int s = tid; s < DN; s += NT) {
         const int gx = wx(x0 - DHH + s % DW), gy = wy(y0 - DHH + s / DW);
@@ -378,7 +383,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
       // ---------------- stage A: post-stream moments on the haloed tile ----
       {
         float4 *slot = ringA + (it % AR) * AV * AN;
-        const int gz = pmod(zA, nz);
+        const int gz = wrapz(zA, nz);
         // D ring: plane zfirst - 1 + j sits in slot j % 3
         const float4 *Dm = ringD + (it % 3) * DN;        // plane zA - 1
         const float4 *D0 = ringD + ((it + 1) % 3) * DN;  // plane zA
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           if (bx >= 1 && bx <= TX && by >= 1 && by <= TY && zB >= z0 && zB < z0 + zc) {
             const int gx = x0 + bx - 1, gy = y0 + by - 1;
             if (gx < nx && gy < ny) {
-              const int i = gx + nx * (gy + ny * pmod(zB, nz));
+              const int i = gx + nx * (gy + ny * wrapz(zB, nz));
               __stcs(DBo + i, n0);
               __stcs(DBo + S + i, n1);
               __stcs(DBo + 2 * S + i, n2);
@@ -489,7 +494,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
       if (zC >= z0 && zC < z0 + zc) {
         const int gx = x0 + tx, gy = y0 + ty;
         if (gx < nx && gy < ny) {
-          const int gz = pmod(zC, nz);
+          const int gz = wrapz(zC, nz);
           Nbr nb;
           make_nbr(nb, gx, gy, gz, nx, ny, nz);
           const int self = noff<18, 1>(nb);
@@ -1144,40 +1149,31 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
                 const double *db, const uint8_t *rockp, cudaStream_t st) {
   const long long N = P.nsites;
   const double rho0 = s.lat.rho0;
-  // rock flag: any rock site present?
-  std::vector<uint8_t> rk(N);
-  if (cudaMemcpyAsync(rk.data(), rockp, N, cudaMemcpyDeviceToHost, st) != cudaSuccess) return LB3DC_ECUDA;
-  cudaStreamSynchronize(st);
-  bool any = false;
-  for (long long i = 0; i < N; ++i) any |= rk[i] != 0;
+  // the caller has uploaded the rock flags (rockp, device) and set any_rock
+  const bool any = P.any_rock != 0;
   if (any && P.nc == 3) return LB3DC_EINVAL;
   if (any && P.le) return LB3DC_ENOTSUP;  // the FP32 Lees-Edwards kernels have no walls
   s.lat = fp32_make_desc(P, rho0, 0, any);
   attach_le(s);
   s.lat.parity = 0;
-  // one FP64 population plane at a time through the staging buffer,
-  // converted to deviations into both buffers
+  // one FP64 plane at a time through the staging buffer: populations
+  // converted to deviations, dipoles rounded to FP32, into both buffers
   cudaError_t e = cudaSuccess;
-  for (int cq = 0; cq < P.nc * 19 && e == cudaSuccess; ++cq) {
-    const double w = (cq % 19 == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
-    e = cudaMemcpyAsync(s.stage, n + (size_t)cq * N, (size_t)N * sizeof(double),
-                        cudaMemcpyHostToDevice, st);
+  const int nplanes = P.nc * 19 + (P.nc == 3 ? 3 : 0);
+  for (int cq = 0; cq < nplanes && e == cudaSuccess; ++cq) {
+    const bool pop = cq < P.nc * 19;
+    const double *src = pop ? n + (size_t)cq * N : db + (size_t)(cq - P.nc * 19) * N;
+    float *d0 = pop ? s.f[0] + (size_t)cq * s.S : s.db[0] + (size_t)(cq - P.nc * 19) * s.S;
+    float *d1 = pop ? s.f[1] + (size_t)cq * s.S : s.db[1] + (size_t)(cq - P.nc * 19) * s.S;
+    const double w = pop ? (cq % 19 == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0 : 0.0;
+    e = cudaMemcpyAsync(s.stage, src, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) break;
-    k_plane_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
-        s.stage, s.f[0] + (size_t)cq * s.S, s.f[1] + (size_t)cq * s.S, N, w, any ? rockp : nullptr);
+    k_plane_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.stage, d0, d1, N, w,
+                                                                    any ? rockp : nullptr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return LB3DC_ECUDA;
-  if (P.nc == 3) {
-    // (ternary lattices have no rock: refused above)
-    std::vector<float> d(3 * N);
-    for (long long i = 0; i < 3 * N; ++i) d[i] = (float)db[i];
-    for (int b = 0; b < 2; ++b)
-      if (cudaMemcpyAsync(s.db[b], d.data(), d.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return LB3DC_ECUDA;
-    cudaStreamSynchronize(st);
-  }
   if (cudaMemcpyAsync(s.d_lat, &s.lat, sizeof(LatDesc), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return LB3DC_ECUDA;
   // keep the launch shape chosen so far (set or autotuned); the kernel

@@ -56,17 +56,16 @@ __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
     float *__restrict__ DBo = (Lg.parity ? db0 : db1) + base;
     const float4 *__restrict__ Mb = Mf + base;
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
-    const bool small = (nx < TX + 2) || (ny < TY + 2);
     const int gx = x0 + tx, gy = y0 + ty;
     const bool act = gx < nx && gy < ny;
     // ring index r holds plane z0 - 1 + r in slot r % RS
     auto load_ring = [&](int r) {
-      const int gz = pmod(z0 - 1 + r, nz);
+      const int gz = wrapz(z0 - 1 + r, nz);
       float4 *slot = sm4 + (r % RS) * AN;
       for (int s = tid; s < AN; s += NT) {
         const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
-        const int ix = small ? pmod(vx, nx) : wrap_small(vx, nx);
-        const int iy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        const int ix = wrapz(vx, nx);
+        const int iy = wrapz(vy, ny);
         cp_async16(slot + s, Mb + ix + nx * (iy + ny * gz));
       }
       if (act)
@@ -87,7 +86,7 @@ __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
         const float3 d = dipole_site<AW>(sm4 + (k % RS) * AN, sm4 + ((k + 1) % RS) * AN,
                                          sm4 + ((k + 2) % RS) * AN, as, Lg, Lg.rho0,
                                          owns[((k + 1) % RS) * NT + tid]);
-        const int i = gx + nx * (gy + ny * pmod(z0 + k, nz));
+        const int i = gx + nx * (gy + ny * wrapz(z0 + k, nz));
         DBo[i] = d.x;
         DBo[S + i] = d.y;
         DBo[2 * S + i] = d.z;
@@ -123,15 +122,14 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
     const uint8_t *__restrict__ RK = rock + base;
     const float rho0 = Lg.rho0, psi0 = Lg.psi0;
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
-    const bool small = (nx < TX + 2) || (ny < TY + 2);
     for (int it = 0; it < zc + 2; ++it) {
-      const int zA = z0 - 1 + it, gz = pmod(zA, nz);
+      const int zA = z0 - 1 + it, gz = wrapz(zA, nz);
       float4 *slotP = ringP + (it % 3) * AN;
       float4 *slotB = ringB + (it % 3) * AN;
       for (int s = tid; s < AN; s += NT) {
         const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
-        const int gx = small ? pmod(vx, nx) : wrap_small(vx, nx);
-        const int gy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        const int gx = wrapz(vx, nx);
+        const int gy = wrapz(vy, ny);
         const int i = gx + nx * (gy + ny * gz);
         if (NC == 3) {
           slotP[s] = __ldg(Mb + S + i);  // {da_z, dpsi_r, dpsi_b, dpsi_s}
@@ -146,7 +144,7 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
         const int gx = x0 + tx, gy = y0 + ty;
         if (gx < nx && gy < ny) {
           const int zC = zA - 1;
-          const int gzc = pmod(zC, nz);
+          const int gzc = wrapz(zC, nz);
           Nbr nb;
           make_nbr(nb, gx, gy, gzc, nx, ny, nz);
           const int self = noff<18, 1>(nb);
@@ -329,18 +327,17 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
     const uint8_t *__restrict__ RK = rock + base;
     const float rho0 = Lg.rho0, psi0 = Lg.psi0;
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
-    const bool small = (nx < TX + 2) || (ny < TY + 2);
     const int gx = x0 + tx, gy = y0 + ty;
     const bool act = gx < nx && gy < ny;
 
     // ring index r holds plane z0 - 1 + r in slot r % RS
     auto load_ring = [&](int r) {
-      const int gz = pmod(z0 - 1 + r, nz);
+      const int gz = wrapz(z0 - 1 + r, nz);
       const int sl = (r % RS) * AN;
       for (int s = tid; s < AN; s += NT) {
         const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
-        const int ix = small ? pmod(vx, nx) : wrap_small(vx, nx);
-        const int iy = small ? pmod(vy, ny) : wrap_small(vy, ny);
+        const int ix = wrapz(vx, nx);
+        const int iy = wrapz(vy, ny);
         const int i = ix + nx * (iy + ny * gz);
         if (NC == 3) {
           cp_async16(ringP4 + sl + s, Mb + S + i);  // {drho_s, dpsi_r, dpsi_b, dpsi_s}
@@ -361,7 +358,7 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
     auto issue_pulls = [&](int k) -> bool {
       if (!act) return true;
       Nbr nb;
-      const int gz = pmod(z0 + k, nz);
+      const int gz = wrapz(z0 + k, nz);
       make_nbr(nb, gx, gy, gz, nx, ny, nz);
       const int self = noff<18, 1>(nb);
       if (ROCK && __ldg(RK + self) != 0) return true;
@@ -390,7 +387,7 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
       cp_async_commit();
       cp_async_wait<2>();  // ring planes up to k + 2 landed (this thread's copies)
       __syncthreads();     // ... and everybody's
-      const int gzc = pmod(z0 + k, nz);
+      const int gzc = wrapz(z0 + k, nz);
       float Fx[NC][3];
       Nbr nb;
       int self = 0;
