@@ -233,7 +233,7 @@ int lb3dc_xdr_write_field(const char *path, const double *v, long long nsites,
  * single-lattice FP32 path.
  */
 typedef struct lb3dc_ensemble lb3dc_ensemble;
-/* capacity_sites bounds the sum of member sizes (19*ncomp*capacity < 2^31);
+/* capacity_sites bounds the sum of member sizes (19*capacity < 2^32);
  * device bytes: 2*19*ncomp*4 (+24 ternary) per site of capacity. */
 int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
                           lb3dc_ensemble **out);

@@ -225,6 +225,8 @@ class Params:
             raise ValueError("invasion boundaries (inv_fluid=%d) are not implemented" % self.inv_fluid)
         if self.boundary_cond > 0:
             raise ValueError("boundary_cond > 0 (generated walls) is not implemented")
+        if self.precision == 1 and 19 * self.nx * self.ny * self.nz >= 1 << 32:
+            raise ValueError("FP32 lattices are limited to 19*sites < 2^32 (226,050,910 sites)")
 
 
 _PARAM_FIELDS = [f.name for f in dataclasses.fields(Params)]

@@ -134,6 +134,9 @@ int validate(const lb3dc_params *p, std::string &why) {
       (long long)p->nx * p->ny * p->nz + 2LL * p->ny * p->nz >= (1LL << 31))
     return (why = "FP64 lattices are limited to 2^31 sites including the Lees-Edwards planes",
             LB3DC_EINVAL);
+  // FP32 population offsets within a component are unsigned 32-bit
+  if (p->precision == LB3DC_FP32_DEV && 19LL * p->nx * p->ny * p->nz >= (1LL << 32))
+    return (why = "FP32 lattices are limited to 19*sites < 2^32 (226,050,910 sites)", LB3DC_EINVAL);
 
   return LB3DC_OK;
 }

@@ -264,8 +264,8 @@ int lb3dc_ensemble_create(int ncomp, long long capacity_sites, int max_lattices,
   if (!out) return efail(nullptr, LB3DC_EINVAL, "out is NULL");
   *out = nullptr;
   if (ncomp != 2 && ncomp != 3) return efail(nullptr, LB3DC_EINVAL, "ncomp must be 2 or 3");
-  if (capacity_sites < 1 || capacity_sites * 19 * ncomp >= (1LL << 31))
-    return efail(nullptr, LB3DC_EINVAL, "capacity must satisfy 19*ncomp*capacity < 2^31 sites");
+  if (capacity_sites < 1 || capacity_sites * 19 >= (1LL << 32))
+    return efail(nullptr, LB3DC_EINVAL, "capacity must satisfy 19*capacity < 2^32 sites");
   if (max_lattices < 1) return efail(nullptr, LB3DC_EINVAL, "max_lattices must be >= 1");
   lb3dc_ensemble *e = new lb3dc_ensemble();
   e->nc = ncomp;

@@ -233,11 +233,13 @@ __device__ __forceinline__ int noff(const Nbr &n) {
 // with code/lb3d_advection.F90:109-151).  F points at component 0 of the
 // lattice; the component stride is 19*S.
 // LAST selects the last-use load hint (the final read of these values by
-// this CTA), which lets L2 drop the lines early.
-template <bool ROCK, bool LAST = false>
-__device__ __forceinline__ void pull_comp(const float *__restrict__ F, int S, int c, const Nbr &n,
+// this CTA), which lets L2 drop the lines early.  NARROW forms the component
+// offset c*19*S in 32 bits (lattices with 19*nc*S < 2^32), which keeps the
+// register-capped moments pass free of 64-bit products.
+template <bool ROCK, bool LAST = false, bool NARROW = false>
+__device__ __forceinline__ void pull_comp(const float *__restrict__ F, unsigned S, int c, const Nbr &n,
                                           int self, const uint8_t *__restrict__ rk, float d[19]) {
-  const float *fc = F + c * 19 * S;
+  const float *fc = NARROW ? F + (unsigned)(c * 19) * S : F + (size_t)(c * 19) * S;
   d[18] = LAST ? __ldlu(fc + 18 * S + self) : __ldg(fc + 18 * S + self);
 #define LB3D_PULL(Q)                                                     \
   {                                                                      \
@@ -269,17 +271,18 @@ __device__ __forceinline__ void make_leyz(LeYZ &w, int gy, int gz, int ny, int n
   w.z[2] = ny * (gz == nz - 1 ? 0 : gz + 1);
 }
 template <int Q>
-__device__ __forceinline__ const float *le_src(const float *fc, int S, int c, const Nbr &n, int gx,
+__device__ __forceinline__ const float *le_src(const float *fc, unsigned S, int c, const Nbr &n, int gx,
                                                int nx, const LeYZ &w, const LatDesc &Lg, int NP) {
   if (cx(Q) == 1 && gx == 0) return Lg.le_h[0] + (c * 19 + Q) * NP + w.y[1 - cy(Q)] + w.z[1 - cz(Q)];
   if (cx(Q) == -1 && gx == nx - 1)
     return Lg.le_h[1] + (c * 19 + Q) * NP + w.y[1 - cy(Q)] + w.z[1 - cz(Q)];
   return fc + Q * S + noff<Q, -1>(n);
 }
-__device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, int S, int c, const Nbr &n,
+template <bool NARROW = false>
+__device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, unsigned S, int c, const Nbr &n,
                                              int self, int gx, int nx, const LeYZ &w,
                                              const LatDesc &Lg, int NP, float d[19]) {
-  const float *fc = F + c * 19 * S;
+  const float *fc = NARROW ? F + (unsigned)(c * 19) * S : F + (size_t)(c * 19) * S;
   d[18] = __ldg(fc + 18 * S + self);
 #define LB3D_PULL_LE(Q) d[Q] = __ldg(le_src<Q>(fc, S, c, n, gx, nx, w, Lg, NP));
   LB3D_PULL_LE(0) LB3D_PULL_LE(1) LB3D_PULL_LE(2) LB3D_PULL_LE(3) LB3D_PULL_LE(4) LB3D_PULL_LE(5)
@@ -290,8 +293,9 @@ __device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, int S,
 
 // ---------------------------------------------------------------------------
 // The fused kernel.  Grid: persistent CTAs over a tile list.  Populations
-// of lattice L live at f[(c*19+q)*S + L.base + site]; offsets are 32-bit,
-// which bounds the packed capacity at 19*nc*S < 2^31.
+// of lattice L live at f[(c*19+q)*S + L.base + site]; each component's
+// base is a 64-bit pointer and the offsets within a component are unsigned
+// 32-bit, which bounds the packed capacity at 19*S < 2^32 sites.
 //
 // On-chip rings (float4 entries, one per site):
 //   A  ternary: {rho_b - rho_r, da_x, da_y, da_z}, {drho_s, dpsi_r, dpsi_b,
@@ -325,10 +329,11 @@ struct FusedGeom {
   static constexpr int SMEM = 16 * (A_F4 + B_F4 + D_F4);
 };
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE, bool LE = false>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE, bool LE = false,
+          bool NARROW = false>
 __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * TY) : (TX * TY >= 512 ? 1 : (TX * TY >= 256 ? 2 : 3))))
     k_fused(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
-            float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, int S,
+            float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock, unsigned S,
             float4 *__restrict__ Mf, float4 *__restrict__ Jf) {
   using G = FusedGeom<NC, TX, TY, MODE>;
   constexpr int NT = G::NT, H = G::H, AW = G::AW, AN = G::AN, AV = G::AV, AR = G::AR;
@@ -402,9 +407,9 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           for (int c = 0; c < NC; ++c) {
             float d[19];
             if constexpr (LE)
-              pull_comp_le(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
+              pull_comp_le<NARROW>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
             else
-              pull_comp<ROCK>(F, S, c, nb, self, RK, d);
+              pull_comp<ROCK, false, NARROW>(F, S, c, nb, self, RK, d);
             if (MODE == MODE_MOMENTS) {
               own_moments<1>(d, dr[c], jm[c][0], jm[c][1], jm[c][2]);
             } else {
@@ -571,7 +576,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
               pull_comp<ROCK, true>(F, S, c, nb, self, RK, d);
               bgk_update(d, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
                          fmaf(k, Fx[c][2], u2), Lg.omega[c]);
-              float *fo = Fo + c * 19 * S + self;
+              float *fo = Fo + (size_t)(c * 19) * S + self;
               // streaming stores: the new populations are not read again in
               // this launch, so they should not displace the inputs from L2
 #pragma unroll
@@ -677,8 +682,11 @@ cudaError_t fp32_from_fp64(const double *n, float *f, long long S, long long bas
 // launch table
 // ---------------------------------------------------------------------------
 constexpr int MODE_DIPOLE = 3, MODE_COLLIDE2 = 4;
+// the moments pass with 32-bit component offsets (k_fused<..., NARROW>)
+constexpr int MODE_MOMENTS32 = 5;
 
 size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
+  if (mode == MODE_MOMENTS32) mode = MODE_MOMENTS;
   const size_t AN1 = (size_t)(sh.tx + 2) * (sh.ty + 2);
   if (mode == MODE_DIPOLE) return 16 * 5 * AN1 + (size_t)4 * 5 * sh.tx * sh.ty;
   if (mode == MODE_COLLIDE2)  // Collide2Geom: ring slots x entry bytes + population stage
@@ -705,6 +713,8 @@ static const void *fused_ptr() {
     return (const void *)k_split_collide2<NC, TX, TY, ROCK, BODY, LE>;
   else if constexpr (MODE == MODE_DIPOLE)
     return (const void *)k_split_dipole<TX, TY>;
+  else if constexpr (MODE == MODE_MOMENTS32)
+    return (const void *)k_fused<NC, TX, TY, ROCK, BODY, MODE_MOMENTS, LE, true>;
   else
     return (const void *)k_fused<NC, TX, TY, ROCK, BODY, MODE, LE>;
 }
@@ -720,9 +730,10 @@ static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
   if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B, MODE, LE>();     \
   if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B, MODE, LE>();
   // the moments and dipole passes do not apply the body force
-  if (MODE == MODE_MOMENTS || MODE == MODE_DIPOLE) body = false;
+  if (MODE == MODE_MOMENTS || MODE == MODE_MOMENTS32 || MODE == MODE_DIPOLE) body = false;
   if constexpr (LE) {
-    static_assert(MODE == MODE_MOMENTS || MODE == MODE_COLLIDE2, "no Lees-Edwards variant");
+    static_assert(MODE == MODE_MOMENTS || MODE == MODE_MOMENTS32 || MODE == MODE_COLLIDE2,
+                  "no Lees-Edwards variant");
     if (nc != 2 || rock) return nullptr;
     if (body) { LB3D_SHAPES(2, false, true) } else { LB3D_SHAPES(2, false, false) }
     return nullptr;
@@ -746,10 +757,12 @@ static const void *kernel_fn(int nc, bool rock, bool body, const FusedShape &sh,
                              bool le = false) {
   if (le) {
     if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS, true>(nc, rock, body, sh);
+    if (mode == MODE_MOMENTS32) return mode_fn<MODE_MOMENTS32, true>(nc, rock, body, sh);
     if (mode == MODE_COLLIDE2) return mode_fn<MODE_COLLIDE2, true>(nc, rock, body, sh);
     return nullptr;
   }
   if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS>(nc, rock, body, sh);
+  if (mode == MODE_MOMENTS32) return mode_fn<MODE_MOMENTS32>(nc, rock, body, sh);
   if (mode == MODE_COLLIDE) return mode_fn<MODE_COLLIDE>(nc, rock, body, sh);
   if (mode == MODE_DIPOLE) return mode_fn<MODE_DIPOLE>(nc, rock, body, sh);
   if (mode == MODE_COLLIDE2) return mode_fn<MODE_COLLIDE2>(nc, rock, body, sh);
@@ -810,7 +823,8 @@ static cudaError_t prepare_kernel(const void *fn, int nthreads, size_t smem, int
 static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const FusedShape &sh,
                                const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                                float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
-                               int S, float4 *M, float4 *J, cudaStream_t st, bool le = false) {
+                               unsigned S, float4 *M, float4 *J, cudaStream_t st, bool le = false) {
+  if (mode == MODE_MOMENTS && 19ull * nc * S < (1ull << 32)) mode = MODE_MOMENTS32;
   const void *fn = kernel_fn(nc, rock, body, sh, mode, le);
   if (!fn) return cudaErrorInvalidConfiguration;
   size_t smem = fp32_mode_smem(nc, sh, mode);
@@ -847,8 +861,8 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
                               float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
                               long long S64, cudaStream_t st, float4 *M, float4 *J,
                               const LEStep *le, const DevParams *P) {
-  if (S64 * 19 * nc >= (1LL << 31)) return cudaErrorInvalidValue;
-  const int S = (int)S64;
+  if (S64 * 19 >= (1LL << 32)) return cudaErrorInvalidValue;
+  const unsigned S = (unsigned)S64;
   if (le) {
     // stage 6 halo, moments pass, stage 8 halo, staged collide pass
     if (!P || nc != 2 || rock || sh.split != 2 || !M) return cudaErrorInvalidValue;

@@ -43,7 +43,7 @@ __device__ __forceinline__ void cp_async_wait() {
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
     k_split_dipole(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
-                   float *db0, float *db1, const float4 *__restrict__ Mf, int S) {
+                   float *db0, float *db1, const float4 *__restrict__ Mf, unsigned S) {
   constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2), RS = 5;
   extern __shared__ float4 sm4[];  // ring [RS][AN] float4, own drho_s [RS][NT] float
   float *owns = reinterpret_cast<float *>(sm4 + RS * AN);
@@ -101,7 +101,7 @@ template <int NC, int TX, int TY, bool ROCK, bool BODY>
 __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
     k_split_collide(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                     float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
-                    int S, const float4 *__restrict__ Mf, const float4 *__restrict__ Jf) {
+                    unsigned S, const float4 *__restrict__ Mf, const float4 *__restrict__ Jf) {
   constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2);
   constexpr int JV = (NC == 3) ? 3 : 2;
   extern __shared__ float4 sm4[];  // psi ring [3][AN], dipole ring [3][AN] (ternary)
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
               pull_comp<ROCK, true>(F, S, c, nb, self, RK, d);
               bgk_update(d, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
                          fmaf(k, Fx[c][2], u2), Lg.omega[c]);
-              float *fo = Fo + c * 19 * S + self;
+              float *fo = Fo + (size_t)(c * 19) * S + self;
 #pragma unroll
               for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
             }
@@ -267,9 +267,9 @@ struct Collide2Geom {
 // Issues the pulls of component c of one site into the stage column
 // (stage[q * NT]), with half-way bounce-back when ROCK (as pull_comp).
 template <bool ROCK, int NT>
-__device__ __forceinline__ void pull_async(const float *__restrict__ F, int S, int c, const Nbr &n,
+__device__ __forceinline__ void pull_async(const float *__restrict__ F, unsigned S, int c, const Nbr &n,
                                            int self, const uint8_t *__restrict__ rk, float *stage) {
-  const float *fc = F + c * 19 * S;
+  const float *fc = F + (size_t)(c * 19) * S;
   cp_async4(stage + 18 * NT, fc + 18 * S + self);
 #define LB3D_APULL(Q)                                                    \
   {                                                                      \
@@ -286,10 +286,10 @@ __device__ __forceinline__ void pull_async(const float *__restrict__ F, int S, i
 
 // pull_async with the Lees-Edwards halo planes across the x boundary
 template <int NT>
-__device__ __forceinline__ void pull_async_le(const float *__restrict__ F, int S, int c, const Nbr &n,
+__device__ __forceinline__ void pull_async_le(const float *__restrict__ F, unsigned S, int c, const Nbr &n,
                                               int self, int gx, int nx, const LeYZ &w,
                                               const LatDesc &Lg, int NP, float *stage) {
-  const float *fc = F + c * 19 * S;
+  const float *fc = F + (size_t)(c * 19) * S;
   cp_async4(stage + 18 * NT, fc + 18 * S + self);
 #define LB3D_APULL_LE(Q) cp_async4(stage + (Q) * NT, le_src<Q>(fc, S, c, n, gx, nx, w, Lg, NP));
   LB3D_APULL_LE(0) LB3D_APULL_LE(1) LB3D_APULL_LE(2) LB3D_APULL_LE(3) LB3D_APULL_LE(4)
@@ -303,7 +303,7 @@ template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false>
 __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
     k_split_collide2(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                      float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
-                     int S, const float4 *__restrict__ Mf) {
+                     unsigned S, const float4 *__restrict__ Mf) {
   using G = Collide2Geom<NC, TX, TY>;
   constexpr int NT = G::NT, AW = G::AW, AN = G::AN, RS = G::RS;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
         }
         if (NC == 3) {
           bgk_update(ds, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1], Lg.omega[NC - 1]);
-          float *fo = Fo + 2 * 19 * S + self;
+          float *fo = Fo + (size_t)38 * S + self;
 #pragma unroll
           for (int q = 0; q < 19; ++q) __stcs(fo + q * S, ds[q]);
         }
@@ -521,7 +521,7 @@ __device__ __forceinline__ double wq64(int q) { return q == 18 ? 1.0 / 3.0 : 1.0
 
 template <int NC>
 __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ lat,
-                           const float *__restrict__ f0, const float *__restrict__ f1, int S) {
+                           const float *__restrict__ f0, const float *__restrict__ f1, unsigned S) {
   const LatDesc &Lg = *lat;
   const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -536,8 +536,8 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) {
         const double w = __dmul_rn(wq64(q), rho0);
-        hb[c][q] = (1.0 - f) * ((double)F[(c * 19 + q) * S + ia] + w) +
-                   f * ((double)F[(c * 19 + q) * S + ib] + w);
+        hb[c][q] = (1.0 - f) * ((double)F[(size_t)(c * 19 + q) * S + ia] + w) +
+                   f * ((double)F[(size_t)(c * 19 + q) * S + ib] + w);
       }
     le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
   }
@@ -547,8 +547,8 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) {
         const double w = __dmul_rn(wq64(q), rho0);
-        ht[c][q] = f * ((double)F[(c * 19 + q) * S + ia] + w) +
-                   (1.0 - f) * ((double)F[(c * 19 + q) * S + ib] + w);
+        ht[c][q] = f * ((double)F[(size_t)(c * 19 + q) * S + ia] + w) +
+                   (1.0 - f) * ((double)F[(size_t)(c * 19 + q) * S + ib] + w);
       }
     le_adjust<NC>(P, ht, hb, L.shear_u, +1.0);
   }
@@ -562,7 +562,7 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
 
 template <int NC>
 __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ lat,
-                            const float *__restrict__ f0, const float *__restrict__ f1, int S) {
+                            const float *__restrict__ f0, const float *__restrict__ f1, unsigned S) {
   const LatDesc &Lg = *lat;
   const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -574,7 +574,7 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
   auto post = [&](int c, int q, int x, int yy, int zz) -> double {
     float v;
     if (q == 18) {
-      v = F[(c * 19 + 18) * S + x + nx * (yy + ny * zz)];
+      v = F[(size_t)(c * 19 + 18) * S + x + nx * (yy + ny * zz)];
     } else {
       const int xu = x - cx(q), yu = pmod(yy - cy(q), ny), zu = pmod(zz - cz(q), nz);
       if (xu < 0)
@@ -582,7 +582,7 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
       else if (xu >= nx)
         v = Lg.le_h[1][(c * 19 + q) * NP + yu + ny * zu];
       else
-        v = F[(c * 19 + q) * S + xu + nx * (yu + ny * zu)];
+        v = F[(size_t)(c * 19 + q) * S + xu + nx * (yu + ny * zu)];
     }
     return (double)v + __dmul_rn(wq64(q), rho0);
   };

@@ -116,3 +116,22 @@ def test_detmath_host_accuracy():
     t = rng.uniform(0.005, 30, 200000)
     assert _ulps(L.detmath_eval("tanh", t), np.tanh(t)).max() <= 3
     assert L.detmath_eval("exp", np.array([0.0, -np.inf, np.inf, 800.0, -800.0])).tolist() == [1.0, 0.0, np.inf, np.inf, 0.0]
+
+
+def test_fp32_size_limit_checked_at_creation():
+    import ctypes
+    from lb3d_b200.config import to_cparams
+    p = Params(nx=620, ny=620, nz=620, ncomp=3, bdist=2).finalize()
+    p.validate()  # FP64 is bounded by memory only
+    p.precision = 1
+    with pytest.raises(ValueError):
+        p.validate()
+    cp = to_cparams(p)
+    h = ctypes.c_void_p()
+    assert L.lib().lb3dc_create(ctypes.byref(cp), ctypes.byref(h)) == L.LB3DC_EINVAL
+    buf = ctypes.create_string_buffer(256)
+    L.lib().lb3dc_last_error(None, buf, 256)
+    assert b"FP32 lattices are limited" in buf.value
+    # the largest FP32 ternary lattice the offsets allow holds 117 GB
+    p2 = Params(nx=608, ny=608, nz=608, ncomp=3, bdist=2, precision=1).finalize()
+    p2.validate()

@@ -128,3 +128,30 @@ def test_async_retire_equals_sync_retire_while_others_step():
     np.testing.assert_array_equal(got_async["db"], got_sync["db"])
     assert e.stats()["resident"] == 1
     e.close()
+
+
+@pytest.mark.parametrize("cap,filler_nz", [(40_000_000, 2300), (80_000_000, 4700)])
+def test_member_beyond_2_31_population_offsets_equals_member_at_base_0(cap, filler_nz):
+    """Ternary ensembles of 40M and 80M sites of capacity (18 and 36 GB of
+    populations): the surfactant populations of a member placed behind a
+    128x128xfiller_nz filler lie beyond 2^31 floats (and, at 80M, beyond 2^32)
+    from the array start; the larger capacity also runs the moments pass with
+    64-bit component offsets.  That member must equal, bit for bit, the same
+    member placed at site 0."""
+    from lb3d_b200.ensemble import Ensemble
+    e = Ensemble(3, capacity_sites=cap, max_lattices=4, shape=(32, 4, 8, 2))
+    try:
+        small = _p((32, 32, 16))
+        a = e.admit(small, seed=7, steps=3)
+        filler = e.admit(_p((128, 128, filler_nz)), seed=8, steps=3)
+        b = e.admit(small, seed=7, steps=3)
+        assert None not in (a, filler, b)
+        while e.stats()["active"]:
+            e.step(1000)
+        ra = e.retire(a, (16, 32, 32))
+        rb = e.retire(b, (16, 32, 32))
+        np.testing.assert_array_equal(ra["n"], rb["n"])
+        np.testing.assert_array_equal(ra["db"], rb["db"])
+        assert np.all(np.isfinite(ra["n"]))
+    finally:
+        e.close()
