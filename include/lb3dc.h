@@ -62,12 +62,16 @@ typedef struct lb3dc_params {
   double rock_colour_r, rock_colour_b;
   int bdist;    /* must be 2 (the third-order equilibrium)               */
   int restore;  /* 1 when the state comes from a checkpoint (init_cond 7) */
-  /* Zou-He flux boundaries on the z planes (boundary_cond != 0 and
-   * inv_fluid = 12, code/lb3d_invasion.F90:2143-2457): inv_type selects the
-   * closure (0, 1 or -1: pr/pg/pb are fluxes rather than velocities), and
-   * pr, pg, pb are the red, surfactant and blue inflow values.            */
+  /* Zou-He boundaries on the z planes (boundary_cond != 0).  Flux
+   * boundaries (inv_fluid = 12, code/lb3d_invasion.F90:2143-2457): inv_type
+   * selects the closure (0, 1 or -1: pr/pg/pb are fluxes rather than
+   * velocities), and pr, pg, pb are the red, surfactant and blue inflow
+   * values.  Density boundaries (inv_fluid = 11, :1459-1796): fr, fb are
+   * the red and blue densities at z = 1, pr, pb those at z = nz.  fr, fg,
+   * fb default to 1.0, 0.1, 0.5 (code/lb3d_config.F90:169).              */
   int inv_type;
   double pr, pg, pb;
+  double fr, fg, fb;
   int precision;/* LB3DC_FP64 or LB3DC_FP32_DEV                           */
   double rho0;  /* reference density of the FP32 deviation storage        */
 } lb3dc_params;

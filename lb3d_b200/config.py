@@ -172,6 +172,9 @@ class Params:
     pr: float = 0.5
     pg: float = 0.1
     pb: float = 1.0
+    fr: float = 1.0
+    fg: float = 0.1
+    fb: float = 0.5
     # product-only fields (not in the reference's namelists)
     precision: int = 0  # 0: FP64 plain drop-in, 1: FP32 deviation storage
     rho0: float = 0.7  # reference density of the FP32 deviation storage
@@ -220,8 +223,12 @@ class Params:
             raise ValueError("only the bdist = 2 equilibrium is implemented")
         if self.psifunc != 2:
             raise ValueError("only psifunc = 2 (psi = 1 - exp(-rho)) is implemented")
+        recolour = self.boundary_cond != 0 and self.inv_fluid in (7, 8)
+        zouhe = self.boundary_cond != 0 and self.inv_fluid in (11, 12)
+        if recolour and self.ncomp != 2:
+            raise ValueError("Illegal value: inv_fluid 7/8 (recolouring) exists in binary builds only")
         if (self.boundary_cond != 0 and self.inv_fluid >= 0 and not self.lees_edwards
-                and self.inv_fluid != 12):
+                and not zouhe and not recolour):
             raise ValueError("invasion boundaries (inv_fluid=%d) are not implemented" % self.inv_fluid)
         if self.boundary_cond > 0:
             raise ValueError("boundary_cond > 0 (generated walls) is not implemented")
@@ -292,7 +299,8 @@ _C_FIELDS = [
     ("rock_colour_r", ctypes.c_double), ("rock_colour_b", ctypes.c_double),
     ("bdist", ctypes.c_int), ("restore", ctypes.c_int),
     ("inv_type", ctypes.c_int), ("pr", ctypes.c_double), ("pg", ctypes.c_double),
-    ("pb", ctypes.c_double),
+    ("pb", ctypes.c_double), ("fr", ctypes.c_double), ("fg", ctypes.c_double),
+    ("fb", ctypes.c_double),
 ]
 
 

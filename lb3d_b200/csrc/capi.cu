@@ -121,7 +121,21 @@ int validate(const lb3dc_params *p, std::string &why) {
     return (why = "the Zou-He flux boundaries need two distinct z planes (nz >= 2)", LB3DC_EINVAL);
   if (zouhe && p->inv_type != 0 && p->inv_type != 1 && p->inv_type != -1)
     return (why = "inv_type must be 0, 1 or -1 for the Zou-He flux boundaries", LB3DC_EINVAL);
-  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && !zouhe)
+  // recolouring inflow, lbe_invade_binary: binary builds only
+  // (code/lb3d_invasion.F90:80-85), on the FP64 path
+  const bool recolour = p->boundary_cond != 0 && (p->inv_fluid == 7 || p->inv_fluid == 8);
+  if (recolour && p->ncomp != 2)
+    return (why = "Illegal value: inv_fluid 7/8 (recolouring) exists in binary builds only", LB3DC_EINVAL);
+  if (recolour && p->precision != LB3DC_FP64)
+    return (why = "the recolouring boundaries run on the FP64 path", LB3DC_ENOTSUP);
+  if (recolour && p->nz < 2)
+    return (why = "the recolouring boundaries need two z planes (nz >= 2)", LB3DC_EINVAL);
+  const bool zh_density = p->boundary_cond != 0 && p->inv_fluid == 11;
+  if (zh_density && p->precision != LB3DC_FP64)
+    return (why = "Zou-He density boundaries run on the FP64 path", LB3DC_ENOTSUP);
+  if (zh_density && p->nz < 2)
+    return (why = "the Zou-He density boundaries need two distinct z planes (nz >= 2)", LB3DC_EINVAL);
+  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && !zouhe && !recolour && !zh_density)
     return (why = "invasion boundaries are not implemented", LB3DC_ENOTSUP);
   if (p->boundary_cond > 0) return (why = "boundary_cond > 0 is not implemented", LB3DC_ENOTSUP);
   if (p->tau_r <= 0 || p->tau_b <= 0 || (p->ncomp == 3 && (p->tau_s <= 0 || p->tau_d <= 0)))
@@ -513,6 +527,16 @@ int lb3dc_bc_apply(lb3dc_handle *h, int stage) {
     if (h->P.zouhe && h->p.precision == LB3DC_FP64) {
       // code/lb3d_bc.F90:125-133: the invasion boundaries come first
       CK(h, fp64_zouhe_flux(h->P, h->g, h->da, h->db, h->rock, h->stream));
+      h->timer.launches += 1;
+    }
+    if (h->p.boundary_cond != 0 && h->p.inv_fluid == 11 && h->p.precision == LB3DC_FP64) {
+      CK(h, fp64_zouhe_density(h->P, h->g, h->rock, h->p.fr, h->p.fb, h->p.pr, h->p.pb, h->stream));
+      h->timer.launches += 1;
+    }
+    if (h->p.boundary_cond != 0 && (h->p.inv_fluid == 7 || h->p.inv_fluid == 8) &&
+        h->p.precision == LB3DC_FP64) {
+      const double mr = h->p.inv_fluid == 7 ? 1.0 : 0.0;
+      CK(h, fp64_recolour(h->P, h->g, h->rock, mr, 1.0 - mr, h->stream));
       h->timer.launches += 1;
     }
     if (h->le && h->p.precision == LB3DC_FP64) {

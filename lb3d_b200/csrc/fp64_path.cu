@@ -320,6 +320,102 @@ __global__ void k_zouhe_flux(DevParams P, double *__restrict__ g, double *__rest
   }
 }
 
+// Zou-He density boundaries, lbe_invade_zouandhe
+// (code/lb3d_invasion.F90:1459-1796): the red and blue populations of the
+// fluid sites of z = 0 take the densities fr, fb, those of z = nz - 1 the
+// densities pr, pb, through the five-population density closure of the
+// non-SINGLEFLUID build (Shan-Chen terms zero).  The velocity closure the
+// reference runs first writes only populations that this closure
+// overwrites, and reads none of them.  F(i) is the reference's 1-based
+// direction i; the blue F(13) at z = 0 divides by amass_r as the reference
+// writes it (:1567).
+__device__ void zouhe_density_site(double *Fp, double rho, double am, double am13, double tau,
+                                   bool bottom) {
+#define F(i) Fp[(i)-1]
+  const double fx = 0.0, fy = 0.0;
+  if (bottom) {
+    F(5) = (-2.0 * F(10) - F(11) - F(12) - 2.0 * F(14) - 2.0 * F(16) - 2.0 * F(18) - F(19) - F(1) -
+            F(2) - F(3) - F(4) + F(6) - F(7) - F(8)) / 3.0 + rho / 3.0 / am;
+    F(9) = (-F(10) + F(11) + F(12) + 2.0 * F(14) - F(16) - F(18) - F(19) / 2.0 - 2.0 * F(1) + F(2) -
+            F(3) / 2.0 - F(4) / 2.0 - F(6) - 2.0 * F(7) - 2.0 * F(8)) / 3.0 + rho / 6.0 / am -
+           fx * tau / 4.0 / am;
+    F(13) = (2.0 * F(10) - 2.0 * F(11) - 2.0 * F(12) - F(14) - F(16) - F(18) - F(19) / 2.0 + F(1) -
+             2.0 * F(2) - F(3) / 2.0 - F(4) / 2.0 - F(6) + F(7) + F(8)) / 3.0 + rho / 6.0 / am13 +
+            fx * tau / 4.0 / am;
+    F(15) = (-F(10) - 2.0 * F(11) + F(12) - F(14) - F(16) + 2.0 * F(18) - F(19) / 2.0 - F(1) / 2.0 -
+             F(2) / 2.0 - 2.0 * F(3) + F(4) - F(6) - 2.0 * F(7) + F(8)) / 3.0 + rho / 6.0 / am -
+            fy * tau / 4.0 / am;
+    F(17) = (-F(10) + F(11) - 2.0 * F(12) - F(14) + 2.0 * F(16) - F(18) - F(19) / 2.0 - F(1) / 2.0 -
+             F(2) / 2.0 + F(3) - 2.0 * F(4) - F(6) + F(7) - 2.0 * F(8)) / 3.0 + rho / 6.0 / am +
+            fy * tau / 4.0 / am;
+  } else {
+    F(6) = (-F(11) - F(12) - 2.0 * F(13) - 2.0 * F(15) - 2.0 * F(17) - F(19) - F(1) - F(2) - F(3) -
+            F(4) + F(5) - F(7) - F(8) - 2.0 * F(9)) / 3.0 + rho / 3.0 / am;
+    F(10) = (F(11) + F(12) + 2.0 * F(13) - F(15) - F(17) - F(19) / 2.0 - 2.0 * F(1) + F(2) -
+             F(3) / 2.0 - F(4) / 2.0 - F(5) - 2.0 * F(7) - 2.0 * F(8) - F(9)) / 3.0 + rho / 6.0 / am -
+            fx * tau / 4.0 / am;
+    F(14) = (-2.0 * F(11) - 2.0 * F(12) - F(13) - F(15) - F(17) - F(19) / 2.0 + F(1) - 2.0 * F(2) -
+             F(3) / 2.0 - F(4) / 2.0 - F(5) + F(7) + F(8) + 2.0 * F(9)) / 3.0 + rho / 6.0 / am +
+            fx * tau / 4.0 / am;
+    F(16) = (-2.0 * F(11) + F(12) - F(13) - F(15) + 2.0 * F(17) - F(19) / 2.0 - F(1) / 2.0 -
+             F(2) / 2.0 - 2.0 * F(3) + F(4) - F(5) - 2.0 * F(7) + F(8) - F(9)) / 3.0 + rho / 6.0 / am -
+            fy * tau / 4.0 / am;
+    F(18) = (F(11) - 2.0 * F(12) - F(13) + 2.0 * F(15) - F(17) - F(19) / 2.0 - F(1) / 2.0 -
+             F(2) / 2.0 + F(3) - 2.0 * F(4) - F(5) + F(7) - 2.0 * F(8) - F(9)) / 3.0 + rho / 6.0 / am +
+            fy * tau / 4.0 / am;
+  }
+#undef F
+}
+
+__global__ void k_zouhe_density(DevParams P, double *__restrict__ g, const uint8_t *__restrict__ rock,
+                                double fr, double fb, double pr, double pb) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const long long N = P.nsites;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * nx * ny) return;
+  const bool bottom = t < nx * ny;
+  const int xy = bottom ? t : t - nx * ny;
+  const int x = xy % nx, y = xy / nx, z = bottom ? 0 : nz - 1;
+  const long long i = sidx(x, y, z, nx, ny);
+  if (rock[i] != 0) return;
+  const double rho_c[2] = {bottom ? fr : pr, bottom ? fb : pb};
+  for (int c = 0; c < 2; ++c) {
+    double F[19];
+    for (int q = 0; q < 19; ++q) F[q] = g[(c * 19 + q) * N + i] * (double)gw(q);
+    zouhe_density_site(F, rho_c[c], P.amass[c], bottom ? P.amass[0] : P.amass[c], P.tau[c], bottom);
+    for (int q = 0; q < 19; ++q) g[(c * 19 + q) * N + i] = F[q] / (double)gw(q);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Recolouring inflow of binary mixtures, lbe_invade_binary
+// (code/lb3d_invasion.F90:1257-1358): on the post-stream populations, the
+// bottom planes z = 0, 1 become red = a * (n_r + n_b), blue = b * (n_r + n_b)
+// with (a, b) = (mr, mb), then the top planes z = nz - 2, nz - 1 with
+// (a, b) = (mb, mr); rock sites are left alone.  One thread per (x, y)
+// column runs the four planes in that order, so lattices with nz < 4, whose
+// bottom and top planes coincide, are recoloured as the reference does.
+// ---------------------------------------------------------------------------
+__global__ void k_recolour(DevParams P, double *__restrict__ g, const uint8_t *__restrict__ rock,
+                           double mr, double mb) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const long long N = P.nsites;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * ny) return;
+  const int x = t % nx, y = t / nx;
+  const int zs[4] = {0, 1, nz - 2, nz - 1};
+  for (int k = 0; k < 4; ++k) {
+    const long long i = sidx(x, y, zs[k], nx, ny);
+    if (rock[i] != 0) continue;
+    const double a = k < 2 ? mr : mb, b = k < 2 ? mb : mr;
+    for (int q = 0; q < 19; ++q) {
+      const double pop = g[q * N + i] + g[(19 + q) * N + i];
+      g[q * N + i] = a * pop;
+      g[(19 + q) * N + i] = b * pop;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Dipole relaxation, code/lb3d_collision.F90:296-403 (ternary, periodic).
 // Reads rho and da of the 18 neighbours; writes db in place (no neighbour
@@ -701,6 +797,20 @@ cudaError_t fp64_zouhe_flux(const DevParams &P, double *g, double *da, const dou
     k_zouhe_flux<2><<<grid_for(n, 128), 128, 0, st>>>(P, g, da, db, rock);
   else
     k_zouhe_flux<3><<<grid_for(n, 128), 128, 0, st>>>(P, g, da, db, rock);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_zouhe_density(const DevParams &P, double *g, const uint8_t *rock, double fr,
+                               double fb, double pr, double pb, cudaStream_t st) {
+  const int n = 2 * P.nx * P.ny;
+  k_zouhe_density<<<grid_for(n, 128), 128, 0, st>>>(P, g, rock, fr, fb, pr, pb);
+  return cudaGetLastError();
+}
+
+cudaError_t fp64_recolour(const DevParams &P, double *g, const uint8_t *rock, double mr, double mb,
+                          cudaStream_t st) {
+  const int n = P.nx * P.ny;
+  k_recolour<<<grid_for(n, 128), 128, 0, st>>>(P, g, rock, mr, mb);
   return cudaGetLastError();
 }
 

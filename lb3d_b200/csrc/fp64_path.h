@@ -11,6 +11,10 @@ cudaError_t fp64_le_halo(const DevParams &P, const LEStep &S, const double *src,
                          cudaStream_t st);
 // Zou-He flux boundaries on the z = 1 and z = nz planes (inv_fluid 12),
 // applied to the post-stream populations g and the advected dipole flux da.
+cudaError_t fp64_zouhe_density(const DevParams &P, double *g, const uint8_t *rock, double fr,
+                               double fb, double pr, double pb, cudaStream_t st);
+cudaError_t fp64_recolour(const DevParams &P, double *g, const uint8_t *rock, double mr, double mb,
+                          cudaStream_t st);
 cudaError_t fp64_zouhe_flux(const DevParams &P, double *g, double *da, const double *db,
                             const uint8_t *rock, cudaStream_t st);
 cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, double *rho,

@@ -657,6 +657,91 @@ struct Oracle {
     }
   }
 
+  // Zou-He density boundaries, lbe_invade_zouandhe
+  // (code/lb3d_invasion.F90:1459-1796), of the red and blue populations at
+  // z = 1 (densities rho_in, :1510-1589) or z = nz (rho_out, :1690-1748),
+  // with the Shan-Chen terms of the non-SINGLEFLUID build set to zero.  The
+  // velocity closure the routine runs first writes only the five
+  // populations that these density formulas then overwrite, and reads none
+  // of them, so it leaves no trace in the result.  F(i) is the reference's
+  // 1-based direction i; am13 is the mass in the rho/6/am term of F(13),
+  // which the reference writes with amass_r for blue as well (:1567).
+  void zouhe_density_site(double *Fp, double rho, double am, double am13, double tau, bool bottom) {
+    auto F = [&](int i) -> double & { return Fp[i - 1]; };
+    const double fx = 0.0, fy = 0.0;
+    if (bottom) {
+      F(5) = (-2.0 * F(10) - F(11) - F(12) - 2.0 * F(14) - 2.0 * F(16) - 2.0 * F(18) - F(19) - F(1) -
+              F(2) - F(3) - F(4) + F(6) - F(7) - F(8)) / 3.0 + rho / 3.0 / am;
+      F(9) = (-F(10) + F(11) + F(12) + 2.0 * F(14) - F(16) - F(18) - F(19) / 2.0 - 2.0 * F(1) + F(2) -
+              F(3) / 2.0 - F(4) / 2.0 - F(6) - 2.0 * F(7) - 2.0 * F(8)) / 3.0 + rho / 6.0 / am -
+             fx * tau / 4.0 / am;
+      F(13) = (2.0 * F(10) - 2.0 * F(11) - 2.0 * F(12) - F(14) - F(16) - F(18) - F(19) / 2.0 + F(1) -
+               2.0 * F(2) - F(3) / 2.0 - F(4) / 2.0 - F(6) + F(7) + F(8)) / 3.0 + rho / 6.0 / am13 +
+              fx * tau / 4.0 / am;
+      F(15) = (-F(10) - 2.0 * F(11) + F(12) - F(14) - F(16) + 2.0 * F(18) - F(19) / 2.0 - F(1) / 2.0 -
+               F(2) / 2.0 - 2.0 * F(3) + F(4) - F(6) - 2.0 * F(7) + F(8)) / 3.0 + rho / 6.0 / am -
+              fy * tau / 4.0 / am;
+      F(17) = (-F(10) + F(11) - 2.0 * F(12) - F(14) + 2.0 * F(16) - F(18) - F(19) / 2.0 - F(1) / 2.0 -
+               F(2) / 2.0 + F(3) - 2.0 * F(4) - F(6) + F(7) - 2.0 * F(8)) / 3.0 + rho / 6.0 / am +
+              fy * tau / 4.0 / am;
+    } else {
+      F(6) = (-F(11) - F(12) - 2.0 * F(13) - 2.0 * F(15) - 2.0 * F(17) - F(19) - F(1) - F(2) - F(3) -
+              F(4) + F(5) - F(7) - F(8) - 2.0 * F(9)) / 3.0 + rho / 3.0 / am;
+      F(10) = (F(11) + F(12) + 2.0 * F(13) - F(15) - F(17) - F(19) / 2.0 - 2.0 * F(1) + F(2) -
+               F(3) / 2.0 - F(4) / 2.0 - F(5) - 2.0 * F(7) - 2.0 * F(8) - F(9)) / 3.0 + rho / 6.0 / am -
+              fx * tau / 4.0 / am;
+      F(14) = (-2.0 * F(11) - 2.0 * F(12) - F(13) - F(15) - F(17) - F(19) / 2.0 + F(1) - 2.0 * F(2) -
+               F(3) / 2.0 - F(4) / 2.0 - F(5) + F(7) + F(8) + 2.0 * F(9)) / 3.0 + rho / 6.0 / am +
+              fx * tau / 4.0 / am;
+      F(16) = (-2.0 * F(11) + F(12) - F(13) - F(15) + 2.0 * F(17) - F(19) / 2.0 - F(1) / 2.0 -
+               F(2) / 2.0 - 2.0 * F(3) + F(4) - F(5) - 2.0 * F(7) + F(8) - F(9)) / 3.0 + rho / 6.0 / am -
+              fy * tau / 4.0 / am;
+      F(18) = (F(11) - 2.0 * F(12) - F(13) + 2.0 * F(15) - F(17) - F(19) / 2.0 - F(1) / 2.0 -
+               F(2) / 2.0 + F(3) - 2.0 * F(4) - F(5) + F(7) - 2.0 * F(8) - F(9)) / 3.0 + rho / 6.0 / am +
+              fy * tau / 4.0 / am;
+    }
+  }
+  void invade_zouhe_density() {
+    for (int plane = 0; plane < 2; ++plane) {
+      const bool bottom = plane == 0;
+      const int z = bottom ? 1 : nz;
+      const double rho_c[2] = {bottom ? p.fr : p.pr, bottom ? p.fb : p.pb};
+      for (int y = 1; y <= ny; ++y)
+        for (int x = 1; x <= nx; ++x) {
+          Site &s = at(x, y, z);
+          if (s.rock != 0.0) continue;
+          for (int c = 0; c < 2; ++c) {
+            double F[19];
+            for (int q = 0; q < 19; ++q) F[q] = s.n[c][q] * (double)G[q];
+            zouhe_density_site(F, rho_c[c], amass[c], bottom ? amass[0] : amass[c], tau[c], bottom);
+            for (int q = 0; q < 19; ++q) s.n[c][q] = F[q] / (double)G[q];
+          }
+        }
+    }
+  }
+
+  // lbe_invade_binary (code/lb3d_invasion.F90:1257-1358), binary builds
+  // (inv_fluid 7: mr = 1, mb = 0; 8: mr = 0, mb = 1): the two bottom planes
+  // z = 1, 2 are recoloured to red = mr * (n_r + n_b), blue = mb * (n_r + n_b)
+  // per population, then the two top planes z = nz - 1, nz the other way
+  // round, skipping rock sites.
+  void invade_recolour(double mr, double mb) {
+    const int zs[4] = {1, 2, nz - 1, nz};
+    for (int k = 0; k < 4; ++k) {
+      const double a = k < 2 ? mr : mb, b = k < 2 ? mb : mr;
+      for (int y = 1; y <= ny; ++y)
+        for (int x = 1; x <= nx; ++x) {
+          Site &s = at(x, y, zs[k]);
+          if (s.rock != 0.0) continue;
+          for (int q = 0; q < 19; ++q) {
+            const double pop = s.n[0][q] + s.n[1][q];
+            s.n[0][q] = a * pop;
+            s.n[1][q] = b * pop;
+          }
+        }
+    }
+  }
+
   void bc_apply(int stage) {
     if (stage == 6) {
       if (le) {
@@ -670,6 +755,9 @@ struct Oracle {
     } else if (stage == 8) {
       // code/lb3d_bc.F90:125-133: invasion first, then the halo exchange
       if (p.boundary_cond != 0 && p.inv_fluid == 12) invade_zouhe_flux();
+      if (p.boundary_cond != 0 && p.inv_fluid == 11) invade_zouhe_density();
+      if (p.boundary_cond != 0 && p.inv_fluid == 7) invade_recolour(1.0, 0.0);
+      if (p.boundary_cond != 0 && p.inv_fluid == 8) invade_recolour(0.0, 1.0);
       exchange();
     }
   }
@@ -705,9 +793,15 @@ void *lb3do_create(const lb3do_params *p) {
   bool le = (p->boundary_cond != 0) && (p->inv_fluid == 5 || p->inv_fluid == 6);
   // code/lb3d_compatibility.F90:105-111: ternary + Lees-Edwards is fatal.
   if (p->ncomp == 3 && le) return nullptr;
-  // Invasion boundaries other than the Lees-Edwards no-ops and the Zou-He
-  // flux boundaries are outside this restatement (code/lb3d_bc.F90:129-133).
-  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && p->inv_fluid != 12) return nullptr;
+  // Invasion boundaries other than the Lees-Edwards no-ops, the Zou-He flux
+  // and density boundaries and the binary recolouring are outside this restatement
+  // (code/lb3d_bc.F90:129-133).  Recolouring exists in binary builds only
+  // (code/lb3d_invasion.F90:80-85) and needs two planes.
+  const bool recolour = p->boundary_cond != 0 && (p->inv_fluid == 7 || p->inv_fluid == 8);
+  if (recolour && (p->ncomp != 2 || p->nz < 2)) return nullptr;
+  const bool zouhe = p->boundary_cond != 0 && (p->inv_fluid == 11 || p->inv_fluid == 12);
+  if (zouhe && p->nz < 2) return nullptr;
+  if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && !zouhe && !recolour) return nullptr;
   Oracle *o = new Oracle();
   o->p = *p;
   o->nx = p->nx;

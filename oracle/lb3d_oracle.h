@@ -41,6 +41,7 @@ typedef struct lb3do_params {
   int restore; /* 1: state came from a checkpoint (init_cond = 7) */
   int inv_type; /* Zou-He closure (inv_fluid = 12) */
   double pr, pg, pb;
+  double fr, fg, fb; /* Zou-He density boundaries (inv_fluid = 11) */
 } lb3do_params;
 
 /* Returns NULL on an unsupported parameter combination. */

@@ -275,6 +275,60 @@ def test_zouhe_flux_boundaries(nc, itype):
         assert_state_equal(lat, o, f"zouHe nc={nc} itype={itype}")
 
 
+@pytest.mark.parametrize("inv_fluid,dims,with_rock", [(7, (10, 7, 9), True), (8, (10, 7, 9), False),
+                                                     (7, (6, 5, 3), False), (8, (6, 5, 2), True)])
+def test_recolouring_boundaries(inv_fluid, dims, with_rock):
+    """Binary recolouring inflow (inv_fluid 7 and 8) on the z planes, with
+    rock sites on the recoloured planes and lattices whose bottom and top
+    planes coincide (nz = 3, 2), bit-identical to the oracle."""
+    p = _params(dims, 2, boundary_cond=-1, inv_fluid=inv_fluid)
+    st = uniform_mixture(*dims, 2, seed=17)
+    if with_rock:
+        rock = np.zeros(dims[::-1])
+        rock[0, 2, 1:4] = 1.0
+        rock[-1, 4, 5] = 1.0
+        st["rock"] = rock
+    lat = _lattice(p, st)
+    o = Oracle(p, st)
+    for _ in range(3):
+        lat.time_loop(4)
+        o.run(4)
+        assert_state_equal(lat, o, f"recolour {inv_fluid} {dims}")
+
+
+@pytest.mark.parametrize("nc,with_rock", [(2, True), (3, False)])
+def test_zouhe_density_boundaries(nc, with_rock):
+    """Zou-He density boundaries on the z planes (inv_fluid 11): red and blue
+    densities fr, fb at z = 1 and pr, pb at z = nz, with unequal masses so
+    the blue F(13) term's amass_r shows, binary with rock sites on the
+    boundary planes and ternary (surfactant untouched), bit-identical to the
+    oracle."""
+    dims = (9, 8, 7)
+    p = _params(dims, nc, boundary_cond=-1, inv_fluid=11, fr=0.75, fb=0.62, pr=0.66, pb=0.71,
+                amass_b=1.3)
+    st = uniform_mixture(*dims, nc, seed=23)
+    if with_rock:
+        rock = np.zeros((7, 8, 9))
+        rock[0, 1, 2:5] = 1.0
+        rock[6, 6, 8] = 1.0
+        rock[3, :, 4] = 1.0
+        st["rock"] = rock
+    lat = _lattice(p, st)
+    o = Oracle(p, st)
+    for _ in range(3):
+        lat.time_loop(4)
+        o.run(4)
+        assert_state_equal(lat, o, f"zouHe density nc={nc}")
+
+
+def test_recolouring_limits():
+    from lb3d_b200.lib import Lattice, Lb3dError
+    with pytest.raises(Lb3dError):
+        Lattice(_params((8, 8, 8), 2, boundary_cond=-1, inv_fluid=7), precision=1)  # FP32: refused
+    with pytest.raises(Lb3dError):
+        Lattice(_params((8, 8, 1), 2, boundary_cond=-1, inv_fluid=8), precision=0)
+
+
 def test_zouhe_limits():
     from lb3d_b200.lib import Lattice, Lb3dError
     p = _params((8, 8, 8), 2, boundary_cond=-1, inv_fluid=12)

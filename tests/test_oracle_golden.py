@@ -8,6 +8,7 @@ device FP64 path uses."""
 import numpy as np
 import pytest
 
+from lb3d_b200.config import Params
 from tests._fixtures import CASES, FIELDS, load_case, load_golden
 from tests._oracle import Oracle, set_math
 
@@ -56,3 +57,73 @@ def test_rejects_fatal_combinations():
     p.boundary_cond, p.inv_fluid = -1, 5  # ternary + Lees-Edwards is fatal
     with pytest.raises(ValueError):
         Oracle(p, st)
+
+
+@pytest.mark.parametrize("inv_fluid", [7, 8])
+def test_recolouring_stage(inv_fluid):
+    """lbe_invade_binary (code/lb3d_invasion.F90:1257-1358) at stage 8: the
+    two bottom planes carry all of n_r + n_b as red (inv_fluid 7) or blue
+    (8), the two top planes the other colour; rock sites and the planes in
+    between are untouched, and every population's n_r + n_b is kept."""
+    from lb3d_b200.ic import uniform_mixture
+    dims = (8, 6, 7)
+    p = Params(nx=8, ny=6, nz=7, ncomp=2, bdist=2, boundary_cond=-1, inv_fluid=inv_fluid,
+               g_br=0.08).finalize()
+    st = uniform_mixture(*dims, 2, seed=3)
+    rock = np.zeros((7, 6, 8))
+    rock[1, 2, 3] = 1.0
+    rock[5, 4, 0] = 1.0
+    st["rock"] = rock
+    o = Oracle(p, st)
+    o.stage(6)
+    o.stage(7)
+    before = o.get()["n"]
+    o.stage(8)
+    after = o.get()["n"]
+    fill, empty = (0, 1) if inv_fluid == 7 else (1, 0)
+    fluid = rock == 0
+    tot = before[0] + before[1]
+    for z in (0, 1):
+        m = fluid[z]
+        assert np.all(after[empty][:, z][:, m] == 0.0)
+        np.testing.assert_array_equal(after[fill][:, z][:, m], tot[:, z][:, m])
+    for z in (5, 6):
+        m = fluid[z]
+        assert np.all(after[fill][:, z][:, m] == 0.0)
+        np.testing.assert_array_equal(after[empty][:, z][:, m], tot[:, z][:, m])
+    np.testing.assert_array_equal(after[:, :, 2:5], before[:, :, 2:5])
+    np.testing.assert_array_equal(after[:, :, 1, 2, 3], before[:, :, 1, 2, 3])
+    np.testing.assert_array_equal(after[:, :, 5, 4, 0], before[:, :, 5, 4, 0])
+
+
+def test_recolouring_is_binary_only():
+    from lb3d_b200.ic import uniform_mixture
+    p = Params(nx=6, ny=6, nz=6, ncomp=3, bdist=2, boundary_cond=-1, inv_fluid=7).finalize()
+    with pytest.raises(ValueError):
+        p.validate()
+    with pytest.raises(ValueError):
+        Oracle(p, uniform_mixture(6, 6, 6, 3, seed=1))
+
+
+def test_zouhe_density_stage_sets_boundary_densities():
+    """lbe_invade_zouandhe (code/lb3d_invasion.F90:1459-1796) at stage 8:
+    the red and blue densities of the fluid sites of z = 1 become fr, fb
+    and those of z = nz become pr, pb (the closure conserves the density it
+    is given; equal masses here), the planes in between are untouched."""
+    from lb3d_b200.ic import uniform_mixture
+    p = Params(nx=7, ny=6, nz=5, ncomp=2, bdist=2, boundary_cond=-1, inv_fluid=11, g_br=0.08,
+               fr=0.8, fb=0.6, pr=0.65, pb=0.75).finalize()
+    st = uniform_mixture(7, 6, 5, 2, seed=4)
+    o = Oracle(p, st)
+    o.stage(6)
+    o.stage(7)
+    before = o.get()["n"]
+    o.stage(8)
+    after = o.get()["n"]
+    g = np.array([2.0] * 6 + [1.0] * 12 + [1.0])  # reference weights: axes 2, rest 1
+    rho = np.einsum("cqzyx,q->czyx", after, g)
+    np.testing.assert_allclose(rho[0, 0], 0.8, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(rho[1, 0], 0.6, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(rho[0, 4], 0.65, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(rho[1, 4], 0.75, rtol=0, atol=1e-14)
+    np.testing.assert_array_equal(after[:, :, 1:4], before[:, :, 1:4])
