@@ -225,6 +225,22 @@ int lb3dc_xdr_write_rock(const char *path, int nx, int ny, int nz, const double 
 int lb3dc_xdr_write_field(const char *path, const double *v, long long nsites,
                           int values_per_site, int dump_double);
 
+/* ---- files written while the lattice keeps stepping -------------------- */
+/* lb3dc_checkpoint_async reads the current state off the device (as
+ * lb3dc_download_state, synchronising) into a pinned buffer of the handle
+ * and returns; a host thread then writes it as lb3dc_xdr_write_checkpoint
+ * does (rock sites with rock_state 1).  lb3dc_dump_async does the same for
+ * one lb3dc_dump field written as lb3dc_xdr_write_field.  One write is in
+ * flight per handle: a new one waits for the previous one first (and
+ * returns its error if it failed); lb3dc_io_wait waits and returns the
+ * status of the last write; lb3dc_destroy waits too.  Replaces the
+ * download + write of lb3d_io_write_checkpoint / lb3d_io_write_data on
+ * dump steps (code/lb3d_time_loop.F90:88-90,
+ * code/lb3d_io_checkpoint.F90:790-873, code/lb3d_io_dump_data.F90:241-301). */
+int lb3dc_checkpoint_async(lb3dc_handle *h, const char *path);
+int lb3dc_dump_async(lb3dc_handle *h, const char *field, const char *path, int dump_double);
+int lb3dc_io_wait(lb3dc_handle *h);
+
 /* ---- ensembles: many lattices, one persistent kernel ------------------- */
 /*
  * Parameter sweeps (many independent small lattices of uneven size) run as

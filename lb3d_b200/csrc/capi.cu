@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lb3dc.h"
@@ -44,6 +45,12 @@ struct lb3dc_handle {
   KernelTimer timer;
   std::string err;
   int errcode = 0;
+  // asynchronous file writers: a pinned host copy of what is being written
+  // and the thread that converts it to XDR and writes the file
+  void *io_pin = nullptr;
+  size_t io_pin_bytes = 0;
+  std::thread io_thread;
+  int io_status = 0;
 };
 
 namespace {
@@ -342,7 +349,9 @@ int lb3dc_create(const lb3dc_params *p, lb3dc_handle **out) {
 
 int lb3dc_destroy(lb3dc_handle *h) {
   if (!h) return LB3DC_OK;
+  if (h->io_thread.joinable()) h->io_thread.join();
   cudaSetDevice(h->device);
+  if (h->io_pin) cudaFreeHost(h->io_pin);
   if (h->stream) cudaStreamSynchronize(h->stream);
   double *bufs[] = {h->f, h->g, h->rho, h->psi, h->mom, h->da, h->db, h->hlo, h->hhi,
                     h->rlo, h->rhi, h->plo, h->phi, h->scratch};
@@ -769,6 +778,81 @@ int lb3dc_dump(lb3dc_handle *h, const char *field, double *out) {
   CK(h, cudaMemcpyAsync(out, h->scratch, (size_t)N * vps * 8, cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   return LB3DC_OK;
+}
+
+// ---- asynchronous checkpoint and dump files --------------------------------
+// The state (or field) is read off the device into a pinned host buffer
+// owned by the handle, synchronously; the big-endian conversion and the
+// file write run on a host thread while the caller keeps stepping.  One
+// write is in flight per handle: a new one first waits for the previous one
+// and, if that failed, returns its error instead of starting.
+static int io_join(lb3dc_handle *h) {
+  if (h->io_thread.joinable()) h->io_thread.join();
+  const int s = h->io_status;
+  h->io_status = LB3DC_OK;
+  return s;
+}
+
+static int io_pinned(lb3dc_handle *h, size_t bytes) {
+  if (h->io_pin_bytes >= bytes) return LB3DC_OK;
+  if (h->io_pin) cudaFreeHost(h->io_pin);
+  h->io_pin = nullptr;
+  h->io_pin_bytes = 0;
+  if (cudaHostAlloc(&h->io_pin, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    h->io_pin = nullptr;
+    cudaGetLastError();
+    return fail(h, LB3DC_ENOMEM, "pinned host buffer of %zu bytes for the file writer", bytes);
+  }
+  h->io_pin_bytes = bytes;
+  return LB3DC_OK;
+}
+
+int lb3dc_checkpoint_async(lb3dc_handle *h, const char *path) {
+  int rc = need_loaded(h);
+  if (rc) return rc;
+  if (!path) return fail(h, LB3DC_EINVAL, "path is NULL");
+  if ((rc = io_join(h))) return fail(h, rc, "the previous asynchronous write failed");
+  const size_t N = (size_t)h->P.nsites, nc = (size_t)h->p.ncomp;
+  const size_t nn = nc * 19 * N, n3 = nc == 3 ? 3 * N : 0;
+  if ((rc = io_pinned(h, (nn + 2 * n3 + N) * 8 + N))) return rc;
+  double *n = (double *)h->io_pin, *da = n + nn, *db = da + n3, *rk = db + n3;
+  uint8_t *rb = (uint8_t *)(rk + N);
+  rc = lb3dc_download_state(h, n, nc == 3 ? db : nullptr, nullptr, nullptr, nc == 3 ? da : nullptr);
+  if (rc) return rc;
+  CK(h, cudaMemcpyAsync(rb, h->rock, N, cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  const std::string file(path);
+  const int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
+  h->io_thread = std::thread([h, file, nx, ny, nz, nc, N, n, da, db, rk, rb]() {
+    // rock sites are written with rock_state 1
+    for (size_t i = 0; i < N; ++i) rk[i] = rb[i] ? 1.0 : 0.0;
+    h->io_status = lb3dc_xdr_write_checkpoint(file.c_str(), nx, ny, nz, (int)nc, n,
+                                              nc == 3 ? da : nullptr, nc == 3 ? db : nullptr, rk);
+  });
+  return LB3DC_OK;
+}
+
+int lb3dc_dump_async(lb3dc_handle *h, const char *field, const char *path, int dump_double) {
+  int rc = need_loaded(h);
+  if (rc) return rc;
+  if (!field || !path) return fail(h, LB3DC_EINVAL, "NULL argument");
+  if ((rc = io_join(h))) return fail(h, rc, "the previous asynchronous write failed");
+  const long long N = h->P.nsites;
+  const int vps = (std::strcmp(field, "dir") == 0 || std::strcmp(field, "arr") == 0) ? 3 : 1;
+  if ((rc = io_pinned(h, (size_t)N * vps * 8))) return rc;
+  double *v = (double *)h->io_pin;
+  if ((rc = lb3dc_dump(h, field, v))) return rc;
+  const std::string file(path);
+  h->io_thread = std::thread([h, file, v, N, vps, dump_double]() {
+    h->io_status = lb3dc_xdr_write_field(file.c_str(), v, N, vps, dump_double);
+  });
+  return LB3DC_OK;
+}
+
+int lb3dc_io_wait(lb3dc_handle *h) {
+  if (!h) return LB3DC_EINVAL;
+  const int rc = io_join(h);
+  return rc ? fail(h, rc, "asynchronous file write failed") : LB3DC_OK;
 }
 
 int lb3dc_detmath_eval(int fn, int device, const double *x, double *y, long long n) {

@@ -84,6 +84,9 @@ def lib():
         "lb3dc_sanity": (I, [H, ctypes.POINTER(LL), ctypes.POINTER(LL)]),
         "lb3dc_sanity_velocity": (I, [H, _D, ctypes.POINTER(I), _D, ctypes.POINTER(LL), ctypes.POINTER(LL)]),
         "lb3dc_dump": (I, [H, ctypes.c_char_p, _D]),
+        "lb3dc_checkpoint_async": (I, [H, ctypes.c_char_p]),
+        "lb3dc_dump_async": (I, [H, ctypes.c_char_p, ctypes.c_char_p, I]),
+        "lb3dc_io_wait": (I, [H]),
         "lb3dc_xdr_read_checkpoint": (I, [ctypes.c_char_p, I, I, I, I, _D, _D, _D]),
         "lb3dc_xdr_write_checkpoint": (I, [ctypes.c_char_p, I, I, I, I, _D, _D, _D, _D]),
         "lb3dc_xdr_read_topo": (I, [ctypes.c_char_p, _D]),
@@ -270,6 +273,17 @@ class Lattice:
         out = np.empty(self.nsites * k)
         self._ck(lib().lb3dc_dump(self.h, field.encode(), ptr(out)))
         return out
+
+    def checkpoint_async(self, path):
+        """Starts writing the current state as an XDR checkpoint file; the
+        lattice may keep stepping.  io_wait() reports the outcome."""
+        self._ck(lib().lb3dc_checkpoint_async(self.h, str(path).encode()))
+
+    def dump_async(self, field, path, dump_double=False):
+        self._ck(lib().lb3dc_dump_async(self.h, field.encode(), str(path).encode(), int(bool(dump_double))))
+
+    def io_wait(self):
+        self._ck(lib().lb3dc_io_wait(self.h))
 
     def conservation(self):
         m, u = np.zeros(3), np.zeros(3)
