@@ -5,30 +5,45 @@
 
 // Dipole relaxation of one site (code/lb3d_collision.F90:296-403) from the
 // ring planes of moment entries {rho_b - rho_r, da_x, da_y, da_z} (row
-// stride AW) and the site's own surfactant density deviation.
+// stride AW) and the site's own surfactant density deviation.  The dipole
+// field h = sum_q g_q [-sgn c_q phi_q + da_q - 2 c_q (c_q . da_q)] + da_own
+// is summed over the nine pairs of opposite neighbours (q, bounce(q)), whose
+// c_q terms differ only in sign: per pair the difference of phi and the sum
+// of da enter once.
 template <int AW>
 __device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0, const float4 *Ap,
                                               int as, const LatDesc &Lg, float rho0, float own_drs) {
-  const float sgn = (Lg.g_bs >= 0.0f) ? 1.0f : -1.0f;
   const float4 own0 = A0[as];
-  float hc0 = 0.f, hc1 = 0.f, hc2 = 0.f;
-  float hs0 = own0.y, hs1 = own0.z, hs2 = own0.w;
+  float P0 = 0.f, P1 = 0.f, P2 = 0.f;  // sum g c (phi_q - phi_qbar)
+  float S0 = 0.f, S1 = 0.f, S2 = 0.f;  // sum g (da_q + da_qbar)
+  float B0 = 0.f, B1 = 0.f, B2 = 0.f;  // sum g c (c . (da_q + da_qbar))
   const float isN = 1.0f / fmaxf(rho0 + own_drs, 1.0e-4f);
 #pragma unroll
   for (int q = 0; q < 18; ++q) {
+    if (bounce(q) < q) continue;  // each pair once, from its first member
+    const int qb = bounce(q);
     const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-    const float4 e0 = Aq[as + cx(q) + AW * cy(q)];
+    const float4 *Ab = cz(qb) == 1 ? Ap : (cz(qb) == -1 ? Am : A0);
+    const float4 e = Aq[as + cx(q) + AW * cy(q)];
+    const float4 f = Ab[as + cx(qb) + AW * cy(qb)];
     const float g = (float)gw(q);
-    const float hcm = -sgn * e0.x * g;
-    const float dot2 = 2.0f * (cx(q) * e0.y + cy(q) * e0.z + cz(q) * e0.w);
-    if (cx(q)) hc0 = fmaf(hcm, (float)cx(q), hc0);
-    if (cy(q)) hc1 = fmaf(hcm, (float)cy(q), hc1);
-    if (cz(q)) hc2 = fmaf(hcm, (float)cz(q), hc2);
-    hs0 = fmaf(e0.y - cx(q) * dot2, g, hs0);
-    hs1 = fmaf(e0.z - cy(q) * dot2, g, hs1);
-    hs2 = fmaf(e0.w - cz(q) * dot2, g, hs2);
+    const float dphi = e.x - f.x;
+    const float s0 = e.y + f.y, s1 = e.z + f.z, s2 = e.w + f.w;
+    S0 = fmaf(g, s0, S0);
+    S1 = fmaf(g, s1, S1);
+    S2 = fmaf(g, s2, S2);
+    float t = 0.f;  // c . s
+    if (cx(q)) t = fmaf((float)cx(q), s0, t);
+    if (cy(q)) t = fmaf((float)cy(q), s1, t);
+    if (cz(q)) t = fmaf((float)cz(q), s2, t);
+    if (cx(q)) P0 = fmaf(g * (float)cx(q), dphi, P0), B0 = fmaf(g * (float)cx(q), t, B0);
+    if (cy(q)) P1 = fmaf(g * (float)cy(q), dphi, P1), B1 = fmaf(g * (float)cy(q), t, B1);
+    if (cz(q)) P2 = fmaf(g * (float)cz(q), dphi, P2), B2 = fmaf(g * (float)cz(q), t, B2);
   }
-  const float h0 = hc0 + hs0, h1 = hc1 + hs1, h2 = hc2 + hs2;
+  const float msgn = (Lg.g_bs >= 0.0f) ? -1.0f : 1.0f;
+  const float h0 = fmaf(msgn, P0, fmaf(-2.0f, B0, own0.y + S0));
+  const float h1 = fmaf(msgn, P1, fmaf(-2.0f, B1, own0.z + S1));
+  const float h2 = fmaf(msgn, P2, fmaf(-2.0f, B2, own0.w + S2));
   const float hn = sqrtf(fmaf(h2, h2, fmaf(h1, h1, h0 * h0)));
   const float hm = Lg.beta * hn;
   const float fac = (hm > 1.0e-2f) ? Lg.d0 * langevin(hm) / hn : Lg.d0 * Lg.beta * (1.0f / 3.0f);
