@@ -58,19 +58,24 @@ __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
     const int gx = x0 + tx, gy = y0 + ty;
     const bool act = gx < nx && gy < ny;
+    // the in-plane offsets of this thread's ring entries, once per tile
+    constexpr int RE = (AN + NT - 1) / NT;
+    int rxy[RE];
+#pragma unroll
+    for (int e = 0; e < RE; ++e) {
+      const int s = tid + e * NT;
+      rxy[e] = s < AN ? wrapz(x0 - 1 + s % AW, nx) + nx * wrapz(y0 - 1 + s / AW, ny) : 0;
+    }
+    const int own_xy = gx + nx * gy;
     // ring index r holds plane z0 - 1 + r in slot r % RS
     auto load_ring = [&](int r) {
-      const int gz = wrapz(z0 - 1 + r, nz);
+      const float4 *plane = Mb + nx * ny * wrapz(z0 - 1 + r, nz);
       float4 *slot = sm4 + (r % RS) * AN;
-      for (int s = tid; s < AN; s += NT) {
-        const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
-        const int ix = wrapz(vx, nx);
-        const int iy = wrapz(vy, ny);
-        cp_async16(slot + s, Mb + ix + nx * (iy + ny * gz));
-      }
+#pragma unroll
+      for (int e = 0; e < RE; ++e)
+        if (tid + e * NT < AN) cp_async16(slot + tid + e * NT, plane + rxy[e]);
       if (act)
-        cp_async4(owns + (r % RS) * NT + tid,
-                  reinterpret_cast<const float *>(Mb + S + gx + nx * (gy + ny * gz)));
+        cp_async4(owns + (r % RS) * NT + tid, reinterpret_cast<const float *>(plane + S + own_xy));
     };
     load_ring(0);
     load_ring(1);
@@ -86,7 +91,7 @@ __global__ void __launch_bounds__(TX *TY, 1280 / (TX * TY))
         const float3 d = dipole_site<AW>(sm4 + (k % RS) * AN, sm4 + ((k + 1) % RS) * AN,
                                          sm4 + ((k + 2) % RS) * AN, as, Lg, Lg.rho0,
                                          owns[((k + 1) % RS) * NT + tid]);
-        const int i = gx + nx * (gy + ny * wrapz(z0 + k, nz));
+        const int i = own_xy + nx * ny * wrapz(z0 + k, nz);
         DBo[i] = d.x;
         DBo[S + i] = d.y;
         DBo[2 * S + i] = d.z;
@@ -330,15 +335,25 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
     const int gx = x0 + tx, gy = y0 + ty;
     const bool act = gx < nx && gy < ny;
 
+    // the in-plane offsets of this thread's ring entries, once per tile
+    constexpr int RE = (AN + NT - 1) / NT;
+    int rxy[RE];
+#pragma unroll
+    for (int e = 0; e < RE; ++e) {
+      const int s = tid + e * NT;
+      rxy[e] = s < AN ? wrapz(x0 - 1 + s % AW, nx) + nx * wrapz(y0 - 1 + s / AW, ny) : 0;
+    }
     // ring index r holds plane z0 - 1 + r in slot r % RS
     auto load_ring = [&](int r) {
       const int gz = wrapz(z0 - 1 + r, nz);
       const int sl = (r % RS) * AN;
-      for (int s = tid; s < AN; s += NT) {
-        const int vx = x0 - 1 + s % AW, vy = y0 - 1 + s / AW;
-        const int ix = wrapz(vx, nx);
-        const int iy = wrapz(vy, ny);
-        const int i = ix + nx * (iy + ny * gz);
+#pragma unroll
+      for (int e = 0; e < RE; ++e) {
+        const int s = tid + e * NT;
+        if (s >= AN) break;
+        const int vx = x0 - 1 + s % AW;                       // Lees-Edwards halo
+        const int iy = LE ? wrapz(y0 - 1 + s / AW, ny) : 0;   // entries only
+        const int i = rxy[e] + nx * ny * gz;
         if (NC == 3) {
           cp_async16(ringP4 + sl + s, Mb + S + i);  // {drho_s, dpsi_r, dpsi_b, dpsi_s}
           float *b = ringB + 3 * sl + s;
