@@ -319,9 +319,14 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   float *mystage = stage + tid;
 
+  // the tile's lattice descriptor, copied to shared memory once per tile:
+  // the per-site physics constants are then shared loads, not global ones
+  __shared__ LatDesc sLat;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile T = tiles[t];
-    const LatDesc &Lg = lats[T.lat];
+    if (tid == 0) sLat = lats[T.lat];
+    __syncthreads();
+    const LatDesc &Lg = sLat;
     const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
     const int base = (int)Lg.base;
     const int par = Lg.parity;
