@@ -255,13 +255,16 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
 // (float2 for binary), dipole ring [5][3][AN] float (ternary; one plane per
 // axis, so the 4-byte copies into it do not collide in banks), population
 // stage [19*NC][NT] float.
-// Five ring slots (one barrier per plane).  Three CTAs of 128 threads per
-// SM (at most 168 registers) measured faster than four CTAs at 128 registers
-// with a four-slot ring and a second barrier per plane.
+// Five ring slots (one barrier per plane).  Ternary lattices run two CTAs
+// of 128 threads per SM with up to 255 registers: measured faster than
+// three CTAs at 168 registers, which were faster than four at 128 with a
+// four-slot ring (the pass gains more from registers, i.e. independent work
+// per warp, than from warps).  Binary lattices keep three CTAs, which the
+// Lees-Edwards variant needs.
 template <int NC, int TX, int TY>
 struct Collide2Geom {
   static constexpr int NT = TX * TY, AW = TX + 2, AN = AW * (TY + 2);
-  static constexpr int RS = 5, MINB = NT >= 256 ? 2 : 3;
+  static constexpr int RS = 5, MINB = NT >= 256 ? (NC == 3 ? 1 : 2) : (NC == 3 ? 2 : 3);
   static constexpr int PB = (NC == 3) ? 16 : 8;  // psi entry bytes
   static constexpr int P_BYTES = RS * AN * PB;
   static constexpr int B_BYTES = (NC == 3) ? RS * AN * 12 : 0;
