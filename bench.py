@@ -196,7 +196,7 @@ def serving(rank, size, nreq=96, seq_sample=4):
     from lb3d_b200.lib import Lattice
     reqs = partition(sweep_requests(nreq, seed=7), rank, size)
     ens = Ensemble(3, capacity_sites=24_000_000, max_lattices=2048, shape=(32, 4, 8, 2))
-    out = Server(ens, chunk=512, download=True).run(reqs)
+    out = Server(ens, chunk=512, download=True, on_result=lambda r, res: None).run(reqs)
     ens.close()
     seq = {}
     sample = reqs[:seq_sample]

@@ -82,6 +82,12 @@ class PinnedPool:
                 self.free.pop(k)
                 break
         else:
+            # idle blocks too small for this request go back to the system,
+            # so a long stream of mixed sizes keeps the pool near its peak need
+            small = [(c, q) for c, q in self.free if c < count]
+            self.free = [(c, q) for c, q in self.free if c >= count]
+            for _, q in small:
+                _bind().lb3dc_host_free(ctypes.c_void_p(q))
             p = ctypes.c_void_p()
             rc = _bind().lb3dc_host_alloc(ctypes.c_longlong(count * 8), ctypes.byref(p))
             if rc != 0:
@@ -257,20 +263,30 @@ def sweep_requests(n, seed=7, rate=200.0, lmin=16, lmax=96, steps=(500, 5000), n
 class Server:
     """Continuous-batching request loop over one Ensemble.  Finished members
     are retired asynchronously: their results travel to the host while the
-    others step, and a request is done when its results have landed."""
+    others step, and a request is done when its results have landed.
 
-    def __init__(self, ensemble: Ensemble, chunk=64, download=True):
+    on_result(request, result) receives each result as it lands, and the
+    server keeps nothing of it (a long stream of large lattices would
+    otherwise fill host memory); without a callback the result is kept on
+    the request as `request.result`."""
+
+    def __init__(self, ensemble: Ensemble, chunk=64, download=True, on_result=None):
         self.ens = ensemble
         self.chunk = chunk
         self.download = download
+        self.on_result = on_result
 
     def _collect(self, copying, done, clock, wait=False):
         while copying:
             landed = [s for s in list(copying) if self.ens.poll(s)]
             for s in landed:
                 r = copying.pop(s)
-                r.result = self.ens.collect(s)
+                res = self.ens.collect(s)
                 r.done = clock()
+                if self.on_result is not None:
+                    self.on_result(r, res)
+                else:
+                    r.result = res
                 done.append(r)
             if not wait or not copying:
                 return

@@ -106,3 +106,18 @@ def test_server_asynchronous_retire_frees_ranges_only_after_landing():
     assert all(r.result is not None and r.done >= r.admitted for r in reqs)
     assert fake.free == [(0, 2 * 32 ** 3)]
     assert not getattr(fake, "copying", {})
+
+
+def test_server_hands_results_to_the_callback_and_keeps_none():
+    """A long request stream must not accumulate results in the server: with
+    on_result each result goes to the callback as it lands and none stays on
+    its request."""
+    reqs = sweep_requests(25, seed=6, rate=1e6, lmin=16, lmax=32, steps=(10, 40))
+    fake = FakeEnsemble(capacity=2 * 32 ** 3)
+    got = []
+    out = Server(fake, chunk=8, download=True,
+                 on_result=lambda r, res: got.append((r.rid, res is not None))).run(reqs, realtime=False)
+    assert out["solves"] == 25
+    assert sorted(g[0] for g in got) == sorted(r.rid for r in reqs)
+    assert all(ok for _, ok in got)
+    assert all(getattr(r, "result", None) is None for r in reqs)
