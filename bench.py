@@ -40,7 +40,7 @@ BYTES_PER_SITE = {("f32", 3): 480, ("f32", 2): 304, ("f64", 3): 960, ("f64", 2):
 # the ternary 128^3 workload, keyed by (tile x, tile y, strategy); captured
 # with 8-plane chunks (the chunk depth moves only the ring halo reloads,
 # under 1 % of this figure).
-NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 774}
+NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 772}
 PHYS = dict(tau_d=1.0, g_br=0.08, g_bs=-0.006, g_ss=-0.0045, beta=10.0, d_0=1.0, bdist=2, restore=1)
 
 
