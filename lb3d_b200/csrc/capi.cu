@@ -122,24 +122,18 @@ int validate(const lb3dc_params *p, std::string &why) {
   if (p->ncomp == 3 && le)
     return (why = "FATAL: Lees Edwards BC are not supported for ternary mixtures", LB3DC_EINVAL);
   const bool zouhe = p->boundary_cond != 0 && p->inv_fluid == 12;
-  if (zouhe && p->precision != LB3DC_FP64)
-    return (why = "Zou-He flux boundaries run on the FP64 path", LB3DC_ENOTSUP);
   if (zouhe && p->nz < 2)
     return (why = "the Zou-He flux boundaries need two distinct z planes (nz >= 2)", LB3DC_EINVAL);
   if (zouhe && p->inv_type != 0 && p->inv_type != 1 && p->inv_type != -1)
     return (why = "inv_type must be 0, 1 or -1 for the Zou-He flux boundaries", LB3DC_EINVAL);
   // recolouring inflow, lbe_invade_binary: binary builds only
-  // (code/lb3d_invasion.F90:80-85), on the FP64 path
+  // (code/lb3d_invasion.F90:80-85)
   const bool recolour = p->boundary_cond != 0 && (p->inv_fluid == 7 || p->inv_fluid == 8);
   if (recolour && p->ncomp != 2)
     return (why = "Illegal value: inv_fluid 7/8 (recolouring) exists in binary builds only", LB3DC_EINVAL);
-  if (recolour && p->precision != LB3DC_FP64)
-    return (why = "the recolouring boundaries run on the FP64 path", LB3DC_ENOTSUP);
   if (recolour && p->nz < 2)
     return (why = "the recolouring boundaries need two z planes (nz >= 2)", LB3DC_EINVAL);
   const bool zh_density = p->boundary_cond != 0 && p->inv_fluid == 11;
-  if (zh_density && p->precision != LB3DC_FP64)
-    return (why = "Zou-He density boundaries run on the FP64 path", LB3DC_ENOTSUP);
   if (zh_density && p->nz < 2)
     return (why = "the Zou-He density boundaries need two distinct z planes (nz >= 2)", LB3DC_EINVAL);
   if (p->boundary_cond != 0 && p->inv_fluid >= 0 && !le && !zouhe && !recolour && !zh_density)
@@ -209,6 +203,11 @@ DevParams make_dev_params(const lb3dc_params &p) {
   P.zh_uz[0] = p.pr;
   P.zh_uz[1] = p.pb;
   P.zh_uz[2] = p.pg;
+  P.invk = p.boundary_cond == 0 ? 0
+           : (p.inv_fluid == 7 || p.inv_fluid == 8) ? 1
+           : p.inv_fluid == 11 ? 2 : p.inv_fluid == 12 ? 3 : 0;
+  P.zh_in[0] = p.fr;
+  P.zh_in[1] = p.fb;
   return P;
 }
 

@@ -50,6 +50,11 @@ struct DevParams {
   int zouhe;          // Zou-He flux boundaries on the z planes (inv_fluid 12)
   int inv_type;       // their closure: 0, 1 or -1 (flux / density)
   double zh_uz[3];    // their inflow per component: red pr, blue pb, surfactant pg
+  // stage-8 inflow kind (boundary_cond != 0): 0 none, 1 recolouring
+  // (inv_fluid 7, 8), 2 Zou-He density (11), 3 Zou-He flux (12); the density
+  // boundaries impose fr, fb at z = 1 (zh_in) and pr, pb at z = nz (zh_uz)
+  int invk;
+  double zh_in[2];
 };
 
 // Per-step Lees-Edwards values, computed on the host in FP64 exactly as

@@ -305,6 +305,65 @@ __device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, unsign
 //   D  ternary: previous dipoles on the tile + 3 halo, 3 planes
 // ---------------------------------------------------------------------------
 #include "fp32_stencil.cuh"
+#include "inflow.cuh"
+
+// Stage-8 inflow boundaries of one site on the FP32 path
+// (code/lb3d_bc.F90:125-133 runs them between advection and collision):
+// applied to the site's post-stream deviations after its own moments were
+// taken, as the reference's collision keeps the advection moments.  Each
+// closure works on the populations n = d + w rho0 in FP32 and writes the
+// deviations back.  Recolouring (code/lb3d_invasion.F90:1257-1358) visits
+// z = 0, 1 and then z = nz - 2, nz - 1 in that order, so planes that are
+// both are recoloured twice as the reference's two loops do; the Zou-He
+// closures (inflow.cuh) act on z = 0 and z = nz - 1 per component,
+// surfactant first.
+template <int NC>
+__device__ __forceinline__ void inflow_site(float2 d01[19], float ds[19], const LatDesc &Lg, int gz,
+                                            int nz) {
+  const float r0 = Lg.rho0;
+  if (Lg.invk == 1) {
+    const float mr = Lg.inv_fluid == 7 ? 1.0f : 0.0f, mb = 1.0f - mr;
+    const int zs[4] = {0, 1, nz - 2, nz - 1};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (gz != zs[k]) continue;
+      const float a = k < 2 ? mr : mb, b = k < 2 ? mb : mr;
+#pragma unroll
+      for (int q = 0; q < 19; ++q) {
+        const float w = wq(q) * r0;
+        const float pop = (d01[q].x + w) + (d01[q].y + w);
+        d01[q].x = a * pop - w;
+        d01[q].y = b * pop - w;
+      }
+    }
+    return;
+  }
+  const bool bottom = gz == 0;
+  if (!bottom && gz != nz - 1) return;
+  float F[19];
+  if (NC == 3 && Lg.invk == 3) {
+#pragma unroll
+    for (int q = 0; q < 19; ++q) F[q] = (ds[q] + wq(q) * r0) * (float)gw(q);
+    zouhe_flux_site<float>(F, Lg.zh_uz[2], bottom, Lg.inv_type);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) ds[q] = F[q] / (float)gw(q) - wq(q) * r0;
+  }
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll
+    for (int q = 0; q < 19; ++q) F[q] = ((c ? d01[q].y : d01[q].x) + wq(q) * r0) * (float)gw(q);
+    if (Lg.invk == 3)
+      zouhe_flux_site<float>(F, Lg.zh_uz[c], bottom, Lg.inv_type);
+    else
+      zouhe_density_site<float>(F, bottom ? Lg.zh_in[c] : Lg.zh_uz[c], Lg.amass[c],
+                                bottom ? Lg.amass[0] : Lg.amass[c], Lg.tau[c], bottom);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+      const float d = F[q] / (float)gw(q) - wq(q) * r0;
+      if (c) d01[q].y = d; else d01[q].x = d;
+    }
+  }
+}
 
 // Kernel modes.  FUSED: one pass per step (moments recomputed on the halo).
 // MOMENTS + COLLIDE: the split strategy, two passes per step: MOMENTS
@@ -419,6 +478,17 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
               dr[c] = acc;
             }
             if (NC == 3 && c == 2) {
+              // Zou-He flux boundaries change the surfactant's populations on
+              // the z planes before its advected dipole flux is summed
+              // (code/lb3d_invasion.F90:2143-2457 recomputes it there)
+              if (MODE == MODE_MOMENTS && Lg.invk == 3 && (gz == 0 || gz == nz - 1)) {
+                float Fs[19];
+#pragma unroll
+                for (int q = 0; q < 19; ++q) Fs[q] = (d[q] + wq(q) * rho0) * (float)gw(q);
+                zouhe_flux_site<float>(Fs, Lg.zh_uz[2], gz == 0, Lg.inv_type);
+#pragma unroll
+                for (int q = 0; q < 19; ++q) d[q] = Fs[q] / (float)gw(q) - wq(q) * rho0;
+              }
               // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
               // (code/lb3d_advection.F90:137-148)
               const int ds0 = (ax + 1) + DW * (ay + 1);  // A-local -> D-local
@@ -705,12 +775,12 @@ size_t fp32_mode_smem(int nc, const FusedShape &sh, int mode) {
 }
 size_t fp32_fused_smem(int nc, const FusedShape &sh) { return fp32_mode_smem(nc, sh, MODE_FUSED); }
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE, bool LE>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, int MODE, bool LE, bool INF = false>
 static const void *fused_ptr() {
   if constexpr (MODE == MODE_COLLIDE)
     return (const void *)k_split_collide<NC, TX, TY, ROCK, BODY>;
   else if constexpr (MODE == MODE_COLLIDE2)
-    return (const void *)k_split_collide2<NC, TX, TY, ROCK, BODY, LE>;
+    return (const void *)k_split_collide2<NC, TX, TY, ROCK, BODY, LE, INF>;
   else if constexpr (MODE == MODE_DIPOLE)
     return (const void *)k_split_dipole<TX, TY>;
   else if constexpr (MODE == MODE_MOMENTS32)
@@ -721,14 +791,15 @@ static const void *fused_ptr() {
 
 // LE: the Lees-Edwards variants, built for binary lattices without rock and
 // only for the moments and staged collide passes (strategy 2).
-template <int MODE, bool LE = false>
+// INF: the staged collide variant with the stage-8 inflow boundaries.
+template <int MODE, bool LE = false, bool INF = false>
 static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
-#define LB3D_SHAPES(NC, R, B)                                                       \
-  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B, MODE, LE>();     \
-  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B, MODE, LE>();     \
-  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B, MODE, LE>();   \
-  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B, MODE, LE>();     \
-  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B, MODE, LE>();
+#define LB3D_SHAPES(NC, R, B)                                                            \
+  if (sh.tx == 32 && sh.ty == 8) return fused_ptr<NC, 32, 8, R, B, MODE, LE, INF>();     \
+  if (sh.tx == 32 && sh.ty == 4) return fused_ptr<NC, 32, 4, R, B, MODE, LE, INF>();     \
+  if (sh.tx == 16 && sh.ty == 16) return fused_ptr<NC, 16, 16, R, B, MODE, LE, INF>();   \
+  if (sh.tx == 16 && sh.ty == 8) return fused_ptr<NC, 16, 8, R, B, MODE, LE, INF>();     \
+  if (sh.tx == 64 && sh.ty == 4) return fused_ptr<NC, 64, 4, R, B, MODE, LE, INF>();
   // the moments and dipole passes do not apply the body force
   if (MODE == MODE_MOMENTS || MODE == MODE_MOMENTS32 || MODE == MODE_DIPOLE) body = false;
   if constexpr (LE) {
@@ -754,7 +825,8 @@ static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
 }
 
 static const void *kernel_fn(int nc, bool rock, bool body, const FusedShape &sh, int mode,
-                             bool le = false) {
+                             bool le = false, bool inf = false) {
+  if (inf && mode == MODE_COLLIDE2) return mode_fn<MODE_COLLIDE2, false, true>(nc, rock, body, sh);
   if (le) {
     if (mode == MODE_MOMENTS) return mode_fn<MODE_MOMENTS, true>(nc, rock, body, sh);
     if (mode == MODE_MOMENTS32) return mode_fn<MODE_MOMENTS32, true>(nc, rock, body, sh);
@@ -823,9 +895,10 @@ static cudaError_t prepare_kernel(const void *fn, int nthreads, size_t smem, int
 static cudaError_t launch_mode(int mode, int nc, bool rock, bool body, const FusedShape &sh,
                                const LatDesc *d_lat, const Tile *d_tiles, int ntiles, int max_grid,
                                float *f0, float *f1, float *db0, float *db1, const uint8_t *rockp,
-                               unsigned S, float4 *M, float4 *J, cudaStream_t st, bool le = false) {
+                               unsigned S, float4 *M, float4 *J, cudaStream_t st, bool le = false,
+                               bool inf = false) {
   if (mode == MODE_MOMENTS && 19ull * nc * S < (1ull << 32)) mode = MODE_MOMENTS32;
-  const void *fn = kernel_fn(nc, rock, body, sh, mode, le);
+  const void *fn = kernel_fn(nc, rock, body, sh, mode, le, inf);
   if (!fn) return cudaErrorInvalidConfiguration;
   size_t smem = fp32_mode_smem(nc, sh, mode);
   int resident = 0;
@@ -878,6 +951,9 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
     return launch_mode(MODE_COLLIDE2, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1,
                        db0, db1, rockp, S, M, nullptr, st, true);
   }
+  // lattices with inflow boundaries run the staged collide's inflow variant
+  const bool inf = P && P->invk != 0;
+  if (inf && sh.split != 2) return cudaErrorInvalidValue;
   if (!sh.split)
     return launch_mode(MODE_FUSED, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1, db0,
                        db1, rockp, S, nullptr, nullptr, st);
@@ -891,7 +967,7 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
                     db1, rockp, S, M, J, st);
   if (e != cudaSuccess) return e;
   return launch_mode(sh.split == 2 ? MODE_COLLIDE2 : MODE_COLLIDE, nc, rock, body, sh, d_lat,
-                     d_tiles, ntiles, max_grid, f0, f1, db0, db1, rockp, S, M, J, st);
+                     d_tiles, ntiles, max_grid, f0, f1, db0, db1, rockp, S, M, J, st, false, inf);
 }
 
 cudaError_t fp32_flip_parity(LatDesc *d_lat, int nlat, cudaStream_t st) {
@@ -947,6 +1023,11 @@ LatDesc fp32_make_desc(const DevParams &P, double rho0, long long base, bool roc
   L.amin_z = P.g_accn_min;
   L.amax_z = P.g_accn_max;
   L.inv_fluid = P.inv_fluid;
+  L.invk = P.invk;
+  L.inv_type = P.inv_type;
+  L.zh_in[0] = (float)P.zh_in[0];
+  L.zh_in[1] = (float)P.zh_in[1];
+  for (int c = 0; c < 3; ++c) L.zh_uz[c] = (float)P.zh_uz[c];
   L.rho0 = (float)rho0;
   L.em0 = (float)std::exp(-rho0);
   L.psi0 = (float)(1.0 - std::exp(-rho0));
@@ -1028,8 +1109,9 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
 
 int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
   if (!fused_fn(P.nc, false, false, sh)) return LB3DC_EINVAL;
-  // Lees-Edwards lattices run the staged split strategy only
-  if (s.le_h[0] && sh.split != 2) return LB3DC_ENOTSUP;
+  // Lees-Edwards lattices and lattices with inflow boundaries run the
+  // staged split strategy only
+  if ((s.le_h[0] || s.lat.invk) && sh.split != 2) return LB3DC_ENOTSUP;
   if (sh.split && !s.M) return LB3DC_EINVAL;
   if (sh.split < 0 || sh.split > 2) return LB3DC_EINVAL;
   if (sh.zc < 1) return LB3DC_EINVAL;
@@ -1044,7 +1126,8 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
     if (t[0] > 2 * P.nx && t[0] > 16) continue;
     for (int zc : zcs) {
       if (zc > P.nz && zc != 8) continue;
-      for (int split = P.le ? 2 : 0; split < 3; ++split) out.push_back(FusedShape{t[0], t[1], zc, split});
+      for (int split = (P.le || P.invk) ? 2 : 0; split < 3; ++split)
+        out.push_back(FusedShape{t[0], t[1], zc, split});
     }
   }
   return out;

@@ -30,6 +30,10 @@ struct LatDesc {
   // le_h[0/1] the sheared pre-stream populations below x = 0 / above
   // x = nx - 1, [nc][19][nz][ny] deviations; le_p[0/1] the psi deviations of
   // the post-stream halo sites, [nz][ny] float2 {dpsi_r, dpsi_b}.
+  // stage-8 inflow boundaries on the z planes (single lattices): kind as
+  // DevParams::invk, the Zou-He closure type and the imposed values
+  int invk, inv_type;
+  float zh_in[2], zh_uz[3];
   float *le_h[2];
   float2 *le_p[2];
 };

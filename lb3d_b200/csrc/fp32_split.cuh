@@ -307,7 +307,8 @@ __device__ __forceinline__ void pull_async_le(const float *__restrict__ F, unsig
 #undef LB3D_APULL_LE
 }
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false>
+// INF: the lattice has stage-8 inflow boundaries on its z planes.
+template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false, bool INF = false>
 __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
     k_split_collide2(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                      float *f0, float *f1, float *db0, float *db1, const uint8_t *__restrict__ rock,
@@ -457,6 +458,8 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
 #pragma unroll
           for (int c = 0; c < NC; ++c) rho[c] = rho0 + dr[c];
         }
+        // stage-8 inflow boundaries act on the populations, not on the moments
+        if constexpr (INF) inflow_site<NC>(d01, ds, Lg, gzc, nz);
         if (BODY) {
           const int x1 = gx + 1, y1 = gy + 1, z1 = gzc + 1;
           bool on;

@@ -23,6 +23,7 @@
 #include "common.cuh"
 #include "detmath.h"
 #include "fp64_path.h"
+#include "inflow.cuh"
 #include "le_common.cuh"
 
 namespace lb3d {
@@ -232,57 +233,6 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
 // and velocities keep their advection values, as in the reference.
 // F(i) is the reference's 1-based direction i.
 // ---------------------------------------------------------------------------
-__device__ void zouhe_flux_site(double *Fp, double uz, bool bottom, int itype) {
-  auto F = [&](int i) -> double & { return Fp[i - 1]; };
-  const double ux = 0., uy = 0.;
-  double rho;
-  if (bottom) {
-    if (itype < 0) {
-      rho = F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
-            2. * (F(6) + F(10) + F(14) + F(16) + F(18)) + uz;
-      uz = (rho > 0.) ? uz / rho : 0.;
-    } else {
-      rho = (F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
-             2. * (F(6) + F(10) + F(14) + F(16) + F(18))) /
-            (1. - uz);
-    }
-    F(5) = F(6) + uz * rho / 3.;
-    if (itype == 0) {
-      F(15) = F(18) - (F(3) - F(4)) / 4. + rho * uz / 6.;
-      F(17) = F(16) + (F(3) - F(4)) / 4. + rho * uz / 6.;
-      F(9) = F(14) - (F(1) - F(2)) / 4. + rho * uz / 6.;
-      F(13) = F(10) + (F(1) - F(2)) / 4. + rho * uz / 6.;
-    } else if (itype == 1 || itype == -1) {
-      F(15) = F(18) - (F(7) + F(11) + F(3) - F(8) - F(12) - F(4)) / 2. + uz * rho / 6. + uy * rho / 2.;
-      F(17) = F(16) - (F(8) + F(12) + F(4) - F(7) - F(11) - F(3)) / 2. + uz * rho / 6. - uy * rho / 2.;
-      F(9) = F(14) - (F(7) + F(8) + F(1) - F(11) - F(12) - F(2)) / 2. + uz * rho / 6. + ux * rho / 2.;
-      F(13) = F(10) - (F(11) + F(12) + F(2) - F(7) - F(8) - F(1)) / 2. + uz * rho / 6. - ux * rho / 2.;
-    }
-  } else {
-    if (itype < 0) {
-      rho = F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
-            2. * (F(5) + F(9) + F(13) + F(15) + F(17)) - uz;
-      uz = (rho > 0.) ? uz / rho : 0.;
-    } else {
-      rho = (F(19) + F(1) + F(2) + F(3) + F(4) + F(7) + F(11) + F(12) + F(8) +
-             2. * (F(5) + F(9) + F(13) + F(15) + F(17))) /
-            (uz + 1.);
-    }
-    F(6) = F(5) - uz * rho / 3.;
-    if (itype == 0) {
-      F(18) = F(15) + (F(3) - F(4)) / 4. - rho * uz / 6.;
-      F(16) = F(17) - (F(3) - F(4)) / 4. - rho * uz / 6.;
-      F(14) = F(9) + (F(1) - F(2)) / 4. - rho * uz / 6.;
-      F(10) = F(13) - (F(1) - F(2)) / 4. - rho * uz / 6.;
-    } else if (itype == 1 || itype == -1) {
-      F(18) = F(15) + (F(7) + F(11) + F(3) - F(8) - F(12) - F(4)) / 2. - uz * rho / 6. - uy * rho / 2.;
-      F(16) = F(17) + (F(8) + F(12) + F(4) - F(7) - F(11) - F(3)) / 2. - uz * rho / 6. + uy * rho / 2.;
-      F(14) = F(9) + (F(7) + F(8) + F(1) - F(11) - F(12) - F(2)) / 2. - uz * rho / 6. - ux * rho / 2.;
-      F(10) = F(13) + (F(11) + F(12) + F(2) - F(7) - F(8) - F(1)) / 2. - uz * rho / 6. + ux * rho / 2.;
-    }
-  }
-}
-
 template <int NC>
 __global__ void k_zouhe_flux(DevParams P, double *__restrict__ g, double *__restrict__ da,
                              const double *__restrict__ db, const uint8_t *__restrict__ rock) {
@@ -329,44 +279,6 @@ __global__ void k_zouhe_flux(DevParams P, double *__restrict__ g, double *__rest
 // overwrites, and reads none of them.  F(i) is the reference's 1-based
 // direction i; the blue F(13) at z = 0 divides by amass_r as the reference
 // writes it (:1567).
-__device__ void zouhe_density_site(double *Fp, double rho, double am, double am13, double tau,
-                                   bool bottom) {
-#define F(i) Fp[(i)-1]
-  const double fx = 0.0, fy = 0.0;
-  if (bottom) {
-    F(5) = (-2.0 * F(10) - F(11) - F(12) - 2.0 * F(14) - 2.0 * F(16) - 2.0 * F(18) - F(19) - F(1) -
-            F(2) - F(3) - F(4) + F(6) - F(7) - F(8)) / 3.0 + rho / 3.0 / am;
-    F(9) = (-F(10) + F(11) + F(12) + 2.0 * F(14) - F(16) - F(18) - F(19) / 2.0 - 2.0 * F(1) + F(2) -
-            F(3) / 2.0 - F(4) / 2.0 - F(6) - 2.0 * F(7) - 2.0 * F(8)) / 3.0 + rho / 6.0 / am -
-           fx * tau / 4.0 / am;
-    F(13) = (2.0 * F(10) - 2.0 * F(11) - 2.0 * F(12) - F(14) - F(16) - F(18) - F(19) / 2.0 + F(1) -
-             2.0 * F(2) - F(3) / 2.0 - F(4) / 2.0 - F(6) + F(7) + F(8)) / 3.0 + rho / 6.0 / am13 +
-            fx * tau / 4.0 / am;
-    F(15) = (-F(10) - 2.0 * F(11) + F(12) - F(14) - F(16) + 2.0 * F(18) - F(19) / 2.0 - F(1) / 2.0 -
-             F(2) / 2.0 - 2.0 * F(3) + F(4) - F(6) - 2.0 * F(7) + F(8)) / 3.0 + rho / 6.0 / am -
-            fy * tau / 4.0 / am;
-    F(17) = (-F(10) + F(11) - 2.0 * F(12) - F(14) + 2.0 * F(16) - F(18) - F(19) / 2.0 - F(1) / 2.0 -
-             F(2) / 2.0 + F(3) - 2.0 * F(4) - F(6) + F(7) - 2.0 * F(8)) / 3.0 + rho / 6.0 / am +
-            fy * tau / 4.0 / am;
-  } else {
-    F(6) = (-F(11) - F(12) - 2.0 * F(13) - 2.0 * F(15) - 2.0 * F(17) - F(19) - F(1) - F(2) - F(3) -
-            F(4) + F(5) - F(7) - F(8) - 2.0 * F(9)) / 3.0 + rho / 3.0 / am;
-    F(10) = (F(11) + F(12) + 2.0 * F(13) - F(15) - F(17) - F(19) / 2.0 - 2.0 * F(1) + F(2) -
-             F(3) / 2.0 - F(4) / 2.0 - F(5) - 2.0 * F(7) - 2.0 * F(8) - F(9)) / 3.0 + rho / 6.0 / am -
-            fx * tau / 4.0 / am;
-    F(14) = (-2.0 * F(11) - 2.0 * F(12) - F(13) - F(15) - F(17) - F(19) / 2.0 + F(1) - 2.0 * F(2) -
-             F(3) / 2.0 - F(4) / 2.0 - F(5) + F(7) + F(8) + 2.0 * F(9)) / 3.0 + rho / 6.0 / am +
-            fx * tau / 4.0 / am;
-    F(16) = (-2.0 * F(11) + F(12) - F(13) - F(15) + 2.0 * F(17) - F(19) / 2.0 - F(1) / 2.0 -
-             F(2) / 2.0 - 2.0 * F(3) + F(4) - F(5) - 2.0 * F(7) + F(8) - F(9)) / 3.0 + rho / 6.0 / am -
-            fy * tau / 4.0 / am;
-    F(18) = (F(11) - 2.0 * F(12) - F(13) + 2.0 * F(15) - F(17) - F(19) / 2.0 - F(1) / 2.0 -
-             F(2) / 2.0 + F(3) - 2.0 * F(4) - F(5) + F(7) - 2.0 * F(8) - F(9)) / 3.0 + rho / 6.0 / am +
-            fy * tau / 4.0 / am;
-  }
-#undef F
-}
-
 __global__ void k_zouhe_density(DevParams P, double *__restrict__ g, const uint8_t *__restrict__ rock,
                                 double fr, double fb, double pr, double pb) {
   const int nx = P.nx, ny = P.ny, nz = P.nz;

@@ -204,3 +204,42 @@ def test_fp32_sanity_velocity_and_sums_on_device():
     mo, uo = o.sums()
     np.testing.assert_allclose(m, mo, rtol=2e-6)
     assert lat.sanity() == (0, 0)
+
+
+@pytest.mark.parametrize("inv_fluid,nc,itype,rock", [
+    (12, 2, 0, True), (12, 2, 1, False), (12, 3, -1, False), (12, 3, 0, False), (12, 3, 1, False),
+    (11, 2, 0, True), (11, 3, 0, False), (7, 2, 0, True), (8, 2, 0, False)])
+def test_fp32_inflow_boundaries(inv_fluid, nc, itype, rock):
+    """The stage-8 inflow boundaries on the FP32 path -- Zou-He flux
+    (inv_fluid 12, every closure), Zou-He density (11) and the binary
+    recolouring (7, 8) -- applied to the staged post-stream deviations of the
+    z planes, against the FP64 oracle within the path's tolerances; binary
+    cases with rock sites on the boundary planes."""
+    dims = (20, 12, 10)
+    p = _params(dims, nc, boundary_cond=-1, inv_fluid=inv_fluid, inv_type=itype, pr=0.01,
+                pb=-0.004, pg=0.002)
+    if inv_fluid == 11:
+        p = _params(dims, nc, boundary_cond=-1, inv_fluid=11, fr=0.75, fb=0.62, pr=0.66, pb=0.71,
+                    amass_b=1.3)
+    st = uniform_mixture(*dims, nc, seed=31)
+    if rock:
+        r = np.zeros(dims[::-1])
+        r[0, 3, 2:6] = 1.0
+        r[-1, 7, 11] = 1.0
+        r[5, :, 9] = 1.0
+        st["rock"] = r
+    lat, a, b, _ = run_both(p, st, 20)
+    check(a, b, nc, f"inflow {inv_fluid} nc={nc} itype={itype}")
+
+
+def test_fp32_inflow_runs_the_staged_split_strategy_only():
+    from lb3d_b200.lib import Lattice, Lb3dError
+    p = _params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=12, pr=0.01, pb=0.0, pg=0.0)
+    lat = Lattice(p, precision=1)
+    lat.upload_state(uniform_mixture(16, 8, 8, 2, seed=1))
+    for split in (0, 1):
+        with pytest.raises(Lb3dError):
+            lat.set_launch_shape(16, 8, 8, split)
+    lat.set_launch_shape(16, 8, 8, 2)
+    lat.autotune()
+    assert lat.launch_shape[3] == 2

@@ -324,15 +324,10 @@ def test_zouhe_density_boundaries(nc, with_rock):
 def test_recolouring_limits():
     from lb3d_b200.lib import Lattice, Lb3dError
     with pytest.raises(Lb3dError):
-        Lattice(_params((8, 8, 8), 2, boundary_cond=-1, inv_fluid=7), precision=1)  # FP32: refused
-    with pytest.raises(Lb3dError):
         Lattice(_params((8, 8, 1), 2, boundary_cond=-1, inv_fluid=8), precision=0)
 
 
 def test_zouhe_limits():
     from lb3d_b200.lib import Lattice, Lb3dError
-    p = _params((8, 8, 8), 2, boundary_cond=-1, inv_fluid=12)
-    with pytest.raises(Lb3dError):
-        Lattice(p, precision=1)  # FP32 path: refused
     with pytest.raises(Lb3dError):
         Lattice(_params((8, 8, 1), 2, boundary_cond=-1, inv_fluid=12), precision=0)
