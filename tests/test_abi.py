@@ -135,3 +135,31 @@ def test_fp32_size_limit_checked_at_creation():
     # the largest FP32 ternary lattice the offsets allow holds 117 GB
     p2 = Params(nx=608, ny=608, nz=608, ncomp=3, bdist=2, precision=1).finalize()
     p2.validate()
+
+
+@pytest.mark.parametrize("kw,text", [
+    (dict(ncomp=3, inv_fluid=7), b"binary builds only"),
+    (dict(ncomp=2, inv_fluid=11, nz=1), b"two distinct z planes"),
+    (dict(ncomp=2, inv_fluid=12, nz=1), b"two distinct z planes"),
+    (dict(ncomp=2, inv_fluid=8, nz=1), b"two z planes"),
+    (dict(ncomp=2, inv_fluid=12, inv_type=2), b"inv_type"),
+    (dict(ncomp=2, inv_fluid=13), b"not implemented"),
+])
+def test_inflow_boundaries_refused_before_device(kw, text):
+    """The stage-8 inflow boundaries' invalid combinations are refused by
+    lb3dc_create with LB3DC_EINVAL or LB3DC_ENOTSUP before any device work,
+    on both paths."""
+    import ctypes
+    from lb3d_b200.config import to_cparams
+    base = dict(nx=8, ny=8, nz=8, bdist=2, boundary_cond=-1)
+    base.update(kw)
+    for precision in (0, 1):
+        p = Params(**base).finalize()
+        p.precision = precision
+        cp = to_cparams(p)
+        h = ctypes.c_void_p()
+        rc = L.lib().lb3dc_create(ctypes.byref(cp), ctypes.byref(h))
+        assert rc in (L.LB3DC_EINVAL, L.LB3DC_ENOTSUP)
+        buf = ctypes.create_string_buffer(256)
+        L.lib().lb3dc_last_error(None, buf, 256)
+        assert text in buf.value, buf.value
