@@ -68,7 +68,8 @@ typedef struct lb3dc_params {
    * velocities), and pr, pg, pb are the red, surfactant and blue inflow
    * values.  Density boundaries (inv_fluid = 11, :1459-1796): fr, fb are
    * the red and blue densities at z = 1, pr, pb those at z = nz.  fr, fg,
-   * fb default to 1.0, 0.1, 0.5 (code/lb3d_config.F90:169).              */
+   * fb default to 1.0, 0.1, 0.5 (code/lb3d_config.F90:169).  Both
+   * precisions; the FP32 path runs them with the staged split strategy.  */
   int inv_type;
   double pr, pg, pb;
   double fr, fg, fb;
@@ -130,8 +131,12 @@ int lb3dc_download_sites(lb3dc_handle *h, double *whole_N);
 int lb3dc_force_apply(lb3dc_handle *h, int stage);
 /* code/lb3d_bc.F90:95-155.  Stage 6 advances the time step counter and,
  * under Lees-Edwards, updates shear_u, shear_sum and the plane offset and
- * builds the x-halo; stage 8 rebuilds the Lees-Edwards halo after
- * streaming.  Periodic halos are an index wrap inside the kernels. */
+ * builds the x-halo; stage 8 applies the inflow boundaries of the z planes
+ * (lbe_invade: Zou-He flux inv_fluid 12, Zou-He density 11, recolouring 7
+ * and 8, code/lb3d_invasion.F90:45-129) and rebuilds the Lees-Edwards halo
+ * after streaming.  On the FP32 path, whose advection is deferred into the
+ * collision's kernel passes, the inflow boundaries run inside those passes.
+ * Periodic halos are an index wrap inside the kernels. */
 int lb3dc_bc_apply(lb3dc_handle *h, int stage);
 /* code/lb3d_advection.F90:40-151 with half-way bounce-back
  * (code/lb3d_bc_bounce.F90:53-90). */
