@@ -56,3 +56,28 @@ def test_sphere_pack_porosity_and_determinism():
     assert abs(1.0 - a.mean() - 0.4) < 0.02
     c = sphere_pack(48, 40, 32, seed=3, porosity=0.4, rmin=4, rmax=7, overlap=False, max_tries=3000)
     assert 1.0 - c.mean() > 0.55  # non-overlapping spheres jam well before
+
+
+def test_inflow_parameters_reach_the_c_struct():
+    """fr, fg, fb and pr, pg, pb (code/lb3d_config.F90:169) and inv_type are
+    read from the namelists with the reference's defaults and travel in
+    lb3dc_params in the order include/lb3dc.h declares."""
+    from lb3d_b200.config import params_from_namelists, to_cparams
+    d = Params()
+    assert (d.fr, d.fg, d.fb) == (1.0, 0.1, 0.5)
+    g = parse_namelists("""
+&fixed_input
+nx = 8, ny = 8, nz = 6
+/
+&variable_input
+boundary_cond = -1, inv_fluid = 11, inv_type = 1, bdist = 2
+fr = 0.75, fb = 0.62, pr = 0.66, pb = 0.71, pg = 0.05
+/
+""")
+    p = params_from_namelists(g, ncomp=2).finalize()
+    p.validate()
+    c = to_cparams(p)
+    assert (c.inv_fluid, c.inv_type) == (11, 1)
+    assert (c.fr, c.fb, c.pr, c.pb, c.pg, c.fg) == (0.75, 0.62, 0.66, 0.71, 0.05, 0.1)
+    names = [n for n, _ in type(c)._fields_]
+    assert names.index("fr") == names.index("pb") + 1 and names.index("precision") == names.index("fb") + 1
