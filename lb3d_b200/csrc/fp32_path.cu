@@ -939,14 +939,16 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
   if (le) {
     // stage 6 halo, moments pass, stage 8 halo, staged collide pass
     if (!P || nc != 2 || rock || sh.split != 2 || !M) return cudaErrorInvalidValue;
-    const unsigned g = (unsigned)((P->ny * P->nz + 127) / 128);
-    k_le_pre32<2><<<g, 128, 0, st>>>(*P, *le, d_lat, f0, f1, S);
+    // one thread per (y, z) of the x-halo planes: 64-thread blocks spread
+    // the few thousand threads over every SM
+    const unsigned g = (unsigned)((P->ny * P->nz + 63) / 64);
+    k_le_pre32<2><<<g, 64, 0, st>>>(*P, *le, d_lat, f0, f1, S);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
       e = launch_mode(MODE_MOMENTS, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1, db0,
                       db1, rockp, S, M, nullptr, st, true);
     if (e != cudaSuccess) return e;
-    k_le_post32<2><<<g, 128, 0, st>>>(*P, *le, d_lat, f0, f1, S);
+    k_le_post32<2><<<g, 64, 0, st>>>(*P, *le, d_lat, f0, f1, S);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return launch_mode(MODE_COLLIDE2, nc, rock, body, sh, d_lat, d_tiles, ntiles, max_grid, f0, f1,
                        db0, db1, rockp, S, M, nullptr, st, true);

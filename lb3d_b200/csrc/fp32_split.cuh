@@ -557,8 +557,8 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
   const double rho0 = (double)Lg.rho0, f = L.lefrac;
   double hb[NC][19], ht[NC][19];
   {
-    const int ia = (nx - 1) + nx * (y + ny * pmod(z + L.eoff, nz));
-    const int ib = (nx - 1) + nx * (y + ny * pmod(z + L.eoff + 1, nz));
+    const int ia = (nx - 1) + nx * (y + ny * wrapz(z + L.eoff, nz));
+    const int ib = (nx - 1) + nx * (y + ny * wrapz(z + L.eoff + 1, nz));
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) {
         const double w = __dmul_rn(wq64(q), rho0);
@@ -568,8 +568,8 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
     le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
   }
   {
-    const int ia = nx * (y + ny * pmod(z - L.eoff - 1, nz));
-    const int ib = nx * (y + ny * pmod(z - L.eoff, nz));
+    const int ia = nx * (y + ny * wrapz(z - L.eoff - 1, nz));
+    const int ib = nx * (y + ny * wrapz(z - L.eoff, nz));
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) {
         const double w = __dmul_rn(wq64(q), rho0);
@@ -602,7 +602,7 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
     if (q == 18) {
       v = F[(size_t)(c * 19 + 18) * S + x + nx * (yy + ny * zz)];
     } else {
-      const int xu = x - cx(q), yu = pmod(yy - cy(q), ny), zu = pmod(zz - cz(q), nz);
+      const int xu = x - cx(q), yu = wrapz(yy - cy(q), ny), zu = wrapz(zz - cz(q), nz);
       if (xu < 0)
         v = Lg.le_h[0][(c * 19 + q) * NP + yu + ny * zu];
       else if (xu >= nx)
@@ -614,14 +614,14 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
   };
   double hb[NC][19], ht[NC][19];
   {
-    const int za = pmod(z + L.eoff, nz), zb = pmod(z + L.eoff + 1, nz);
+    const int za = wrapz(z + L.eoff, nz), zb = wrapz(z + L.eoff + 1, nz);
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q)
         hb[c][q] = (1.0 - f) * post(c, q, nx - 1, y, za) + f * post(c, q, nx - 1, y, zb);
     le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
   }
   {
-    const int za = pmod(z - L.eoff - 1, nz), zb = pmod(z - L.eoff, nz);
+    const int za = wrapz(z - L.eoff - 1, nz), zb = wrapz(z - L.eoff, nz);
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q)
         ht[c][q] = f * post(c, q, 0, y, za) + (1.0 - f) * post(c, q, 0, y, zb);
