@@ -1,11 +1,21 @@
-"""Multi-GPU plumbing: one process per GPU, replicas only.
+"""Multi-GPU plumbing: one process per GPU.
 
-The hot path exchanges no data between independent lattices, so N GPUs run
-N independent lattices (or N disjoint shares of a request stream) with no
-collective on the data path.  torch.distributed is used only to agree on
-timing: a barrier before and after the timed region and the maximum of the
-per-rank device times.  Ranks read RANK / LOCAL_RANK / WORLD_SIZE /
-MASTER_ADDR / MASTER_PORT from the environment (torchrun).
+Replicas: independent lattices exchange no data, so N GPUs run N
+independent lattices (or N disjoint shares of a request stream) with no
+collective on the data path; torch.distributed only agrees on timing (a
+barrier around the timed region and the maximum of the per-rank device
+times).
+
+Slabs: one lattice split along y over the ranks, as the reference splits its
+lattice over MPI ranks (code/lb3d_mpi.F90:492-596).  Each rank owns a
+contiguous range of y planes (y_slab) and, at every halo exchange, sends its
+first plane to the rank below and its last plane to the rank above and
+receives their faces into its y-halo planes (exchange_y_faces), periodic in
+y across the ranks.  The faces travel point to point (NCCL over NVLink on
+GPUs, gloo on the CPU).
+
+Ranks read RANK / LOCAL_RANK / WORLD_SIZE / MASTER_ADDR / MASTER_PORT from
+the environment (torchrun).
 """
 from __future__ import annotations
 
@@ -64,3 +74,38 @@ def sum_over_ranks(values: Sequence[float], device: str = "cpu") -> List[float]:
 def replica_seed(base_seed: int, rank: int) -> int:
     """Seed of a rank's replica lattice: distinct and reproducible."""
     return base_seed + 7919 * rank
+
+
+def y_slab(ny: int, rank: int, size: int) -> tuple:
+    """(y0, planes) of this rank's slab: ny planes split into contiguous
+    ranges that differ in length by at most one (each at least one plane)."""
+    if size < 1 or not (0 <= rank < size) or ny < size:
+        raise ValueError("bad rank/size for the slab split")
+    y0 = ny * rank // size
+    return y0, ny * (rank + 1) // size - y0
+
+
+# message tags of the two faces: a rank's last plane becomes the lower halo
+# of the rank above, its first plane the upper halo of the rank below
+_TAG_TO_ABOVE, _TAG_TO_BELOW = 17, 18
+
+
+def exchange_y_faces(lo, hi, rank: int, size: int, group=None):
+    """Sends this slab's first (lo) and last (hi) y planes to the ranks below
+    and above and returns (lower_halo, upper_halo): the plane below y = 0
+    (the last plane of the rank below) and the plane above the last one (the
+    first plane of the rank above), periodic over the ranks.  lo, hi: torch
+    tensors of one plane each (any device the backend supports)."""
+    import torch
+    import torch.distributed as dist
+    if size == 1:
+        return hi.clone(), lo.clone()
+    below, above = (rank - 1) % size, (rank + 1) % size
+    lower, upper = torch.empty_like(hi), torch.empty_like(lo)
+    ops = [dist.P2POp(dist.isend, hi.contiguous(), above, group, _TAG_TO_ABOVE),
+           dist.P2POp(dist.isend, lo.contiguous(), below, group, _TAG_TO_BELOW),
+           dist.P2POp(dist.irecv, lower, below, group, _TAG_TO_ABOVE),
+           dist.P2POp(dist.irecv, upper, above, group, _TAG_TO_BELOW)]
+    for w in dist.batch_isend_irecv(ops):
+        w.wait()
+    return lower, upper

@@ -107,6 +107,12 @@ void boltz_dist2(double ux, double uy, double uz, double dux, double duy, double
 struct Oracle {
   lb3do_params p;
   int nx, ny, nz, nc;
+  // y-slab of a decomposed lattice: its first plane's global y offset and
+  // the exchange that fills the y-halo planes from the neighbouring slabs
+  // (null: this lattice is periodic in y, as one rank is)
+  int y_off = 0;
+  lb3do_halo_fn yhook = nullptr;
+  void *yctx = nullptr;
   double omega[3], omega_d, amass[3], tau[3];
   std::vector<Site> N, Nbuf;
   std::vector<double> F;  // forces [interior site][comp][3]
@@ -161,11 +167,18 @@ struct Oracle {
         at(0, y, z) = at(nx, y, z);
         at(nx + 1, y, z) = at(1, y, z);
       }
-    for (int z = 1; z <= nz; ++z)
-      for (int x = 0; x <= nx + 1; ++x) {
-        at(x, 0, z) = at(x, ny, z);
-        at(x, ny + 1, z) = at(x, 1, z);
-      }
+    if (yhook) {
+      // the y neighbours are other ranks' slabs (code/lb3d_mpi.F90:492-596
+      // exchanges the y faces after the x faces and before the z faces, so
+      // the planes sent carry their x halo and the z faces copy the y halo)
+      yhook(yctx, this);
+    } else {
+      for (int z = 1; z <= nz; ++z)
+        for (int x = 0; x <= nx + 1; ++x) {
+          at(x, 0, z) = at(x, ny, z);
+          at(x, ny + 1, z) = at(x, 1, z);
+        }
+    }
     for (int y = 0; y <= ny + 1; ++y)
       for (int x = 0; x <= nx + 1; ++x) {
         at(x, y, 0) = at(x, y, nz);
@@ -499,13 +512,14 @@ struct Oracle {
     }
   }
 
-  // lb3d_get_applyforce, code/lb3d_collision.F90:431-460 (one rank: global
-  // coordinates equal local ones).
+  // lb3d_get_applyforce, code/lb3d_collision.F90:431-460, in global
+  // coordinates (a y-slab adds its offset).
   bool applyforce(int x, int y, int z) const {
     if (p.inv_fluid == 9) return (z == 1) || (z == nz);
     if (p.inv_fluid == 20 || p.inv_fluid == 21) return z == 1;
+    const int gy = y + y_off;
     return (z >= p.g_accn_min) && (z <= p.g_accn_max) && (x >= p.g_accn_min_x) &&
-           (x <= p.g_accn_max_x) && (y >= p.g_accn_min_y) && (y <= p.g_accn_max_y);
+           (x <= p.g_accn_max_x) && (gy >= p.g_accn_min_y) && (gy <= p.g_accn_max_y);
   }
 
   // ---- lb3d_collision_step, code/lb3d_collision.F90:59-291 ---------------
@@ -901,6 +915,37 @@ int lb3do_stage(void *h, int stage) {
   }
 }
 
+int lb3do_set_slab(void *h, int y_off, lb3do_halo_fn fn, void *ctx) {
+  Oracle *o = static_cast<Oracle *>(h);
+  if (o->le || y_off < 0) return -1;  // Lees-Edwards lattices are one slab
+  o->y_off = y_off;
+  o->yhook = fn;
+  o->yctx = ctx;
+  return 0;
+}
+
+long long lb3do_yplane_doubles(const void *h) {
+  const Oracle *o = static_cast<const Oracle *>(h);
+  return (long long)(o->nx + 2) * o->nz * (long long)(sizeof(Site) / sizeof(double));
+}
+
+int lb3do_yplane(void *h, int y, double *buf, int put) {
+  Oracle *o = static_cast<Oracle *>(h);
+  if (y < 0 || y > o->ny + 1) return -1;
+  static_assert(sizeof(Site) % sizeof(double) == 0, "Site is a block of doubles");
+  const size_t sd = sizeof(Site) / sizeof(double);
+  for (int z = 1; z <= o->nz; ++z)
+    for (int x = 0; x <= o->nx + 1; ++x) {
+      double *b = buf + ((size_t)(z - 1) * (o->nx + 2) + x) * sd;
+      Site &s = o->at(x, y, z);
+      if (put)
+        std::memcpy(&s, b, sizeof(Site));
+      else
+        std::memcpy(b, &s, sizeof(Site));
+    }
+  return 0;
+}
+
 int lb3do_run(void *h, int nsteps) {
   Oracle *o = static_cast<Oracle *>(h);
   for (int i = 0; i < nsteps; ++i) o->step();
@@ -984,7 +1029,8 @@ int lb3do_dump(void *hh, const char *field, double *out) {
             }
             v = v / fmax_f(10.0e-9, den);
             if ((z >= o->p.g_accn_min) && (z <= o->p.g_accn_max) && (x >= o->p.g_accn_min_x) &&
-                (x <= o->p.g_accn_max_x) && (y >= o->p.g_accn_min_y) && (y <= o->p.g_accn_max_y))
+                (x <= o->p.g_accn_max_x) && (y + o->y_off >= o->p.g_accn_min_y) &&
+                (y + o->y_off <= o->p.g_accn_max_y))
               v = v - o->p.g_accn / 2.0;
             out[i] = v;
           } else {
@@ -1011,7 +1057,8 @@ int lb3do_dump(void *hh, const char *field, double *out) {
             out[3 * i + k] = v / (double)denf;
           }
           if ((z >= o->p.g_accn_min) && (z <= o->p.g_accn_max) && (x >= o->p.g_accn_min_x) &&
-              (x <= o->p.g_accn_max_x) && (y >= o->p.g_accn_min_y) && (y <= o->p.g_accn_max_y)) {
+              (x <= o->p.g_accn_max_x) && (y + o->y_off >= o->p.g_accn_min_y) &&
+                (y + o->y_off <= o->p.g_accn_max_y)) {
             if (s.rock == 0.0) {
               out[3 * i + 0] = out[3 * i + 0] - o->p.g_accn_x / 2.0;
               out[3 * i + 1] = out[3 * i + 1] - o->p.g_accn_y / 2.0;

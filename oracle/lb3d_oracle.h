@@ -82,6 +82,20 @@ int lb3do_sums(const void *h, double mass[3], double mom[3]);
 int lb3do_sanity_velocity(const void *h, double maxvel[9], int maxpos[27], double velsum[9],
                           long long *n_fluid, long long *n_too_fast);
 
+/* y-slab decomposition (code/lb3d_mpi.F90:492-596 splits the lattice over
+ * ranks; here along y only).  A slab oracle is created with ny = its own
+ * planes and global-coordinate parameters; lb3do_set_slab, called before
+ * lb3do_load, gives its first plane's global y offset and the function that
+ * fills the y-halo planes y = 0 and y = ny + 1 from the neighbouring slabs
+ * at every halo exchange (with lb3do_yplane), after the x faces and before
+ * the z faces.  Not for Lees-Edwards lattices. */
+typedef void (*lb3do_halo_fn)(void *ctx, void *h);
+int lb3do_set_slab(void *h, int y_off, lb3do_halo_fn fn, void *ctx);
+/* Doubles in one y plane of whole sites, x = 0..nx+1, z = 1..nz. */
+long long lb3do_yplane_doubles(const void *h);
+/* Copies plane y (0..ny+1) out of (put = 0) or into (put = 1) buf. */
+int lb3do_yplane(void *h, int y, double *buf, int put);
+
 double lb3do_shear_sum(const void *h);
 int lb3do_nt(const void *h);
 

@@ -17,6 +17,7 @@ class OParams(ctypes.Structure):
 
 
 _lib = None
+HALO_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p)
 
 
 def lib():
@@ -38,6 +39,10 @@ def lib():
         L.lb3do_sanity_velocity.argtypes = [V, D, ctypes.POINTER(ctypes.c_int), D,
                                             ctypes.POINTER(ctypes.c_longlong),
                                             ctypes.POINTER(ctypes.c_longlong)]
+        L.lb3do_set_slab.argtypes = [V, I, HALO_FN, V]
+        L.lb3do_yplane_doubles.argtypes = [V]
+        L.lb3do_yplane_doubles.restype = ctypes.c_longlong
+        L.lb3do_yplane.argtypes = [V, I, D, I]
         L.lb3do_shear_sum.argtypes = [V]
         L.lb3do_shear_sum.restype = ctypes.c_double
         L.lb3do_nt.argtypes = [V]
@@ -59,7 +64,11 @@ def _ptr(a):
 class Oracle:
     """One reference-equivalent lattice on the CPU."""
 
-    def __init__(self, p, state, threads=0):
+    def __init__(self, p, state, threads=0, slab=None):
+        """slab = (y_off, exchange): this oracle holds p.ny planes of a
+        lattice split along y, starting at global plane y_off (p carries the
+        global-coordinate parameters); exchange(oracle) fills its y-halo
+        planes from the neighbouring slabs at every halo exchange."""
         L = lib()
         if threads:
             L.lb3do_set_threads(threads)
@@ -70,6 +79,11 @@ class Oracle:
         if not self.h:
             raise ValueError("oracle rejected the parameter set")
         self.p = p
+        if slab is not None:
+            y_off, exchange = slab
+            self._hook = HALO_FN(lambda ctx, h: exchange(self))
+            if L.lb3do_set_slab(self.h, int(y_off), self._hook, None) != 0:
+                raise ValueError("slab rejected")
         n = np.ascontiguousarray(state["n"], dtype=np.float64)
         db = state.get("db")
         db = None if db is None else np.ascontiguousarray(db, dtype=np.float64)
@@ -113,6 +127,16 @@ class Oracle:
         if lib().lb3do_dump(self.h, field.encode(), _ptr(out)) != 0:
             raise ValueError(field)
         return out
+
+    def yplane(self, y):
+        """Whole sites of plane y (0 .. ny + 1), x = 0..nx+1, z = 1..nz, as doubles."""
+        out = np.empty(lib().lb3do_yplane_doubles(self.h))
+        lib().lb3do_yplane(self.h, int(y), _ptr(out), 0)
+        return out
+
+    def set_yplane(self, y, buf):
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        lib().lb3do_yplane(self.h, int(y), _ptr(buf), 1)
 
     def sums(self):
         m = np.zeros(3)
