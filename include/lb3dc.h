@@ -158,8 +158,15 @@ int lb3dc_sync(lb3dc_handle *h);
  * (48 B / 32 B), a dipole pass (ternary) and a collide pass that reads them
  * with their halo, 2 = as 1, but the collide pass stages each site's pulled
  * populations in shared memory with asynchronous copies one plane ahead
- * and sums the own moments itself (no own-moment field).  All strategies
- * give the same result up to FP32 rounding; 1 and 2 agree bit for bit. */
+ * and sums the own moments itself (no own-moment field), 3 = a moments
+ * pass writing halo-padded moment fields, a dipole pass (ternary) and a
+ * collide pass that receive those fields as TMA boxes with a one-site halo,
+ * the collide pass writing the equilibrium: offered only when every
+ * component relaxes fully (tau = 1) on a lattice at least 2 sites across in
+ * x and y without Lees-Edwards planes or inflow boundaries (LB3DC_ENOTSUP
+ * otherwise); each of its passes chunks z to fill its own resident grid, so
+ * zc is not used.  All strategies give the same result up to FP32
+ * rounding; 0, 1, 2 and 3 agree bit for bit (up to the sign of zero). */
 int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc, int split);
 int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc, int *split);
 /* Times every supported shape and strategy on this lattice (on a saved copy
@@ -325,7 +332,8 @@ long long lb3dc_ensemble_bytes(const lb3dc_ensemble *e);
  * lb3dc_last_error(NULL, ...).  Lees-Edwards and FP32 are not offered here.
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  All calls share the one array and it keeps the last call's
+ * capture; the address is kept per device and context, and looked up again
+ * (outside any capture, too) after a device reset.  All calls share the one array and it keeps the last call's
  * contents: calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialised by the caller.  Asynchronous on
  * `stream`; returns after enqueueing. */

@@ -622,6 +622,10 @@ int lb3dc_sync(lb3dc_handle *h) {
   cudaSetDevice(h->device);
   CK(h, cudaStreamSynchronize(h->stream));
   CK(h, cudaGetLastError());
+  if (h->p.precision == LB3DC_FP32_DEV) {
+    const int rc = fp32_take_error(h->s32, h->stream);
+    if (rc) return fail(h, rc, "a bounded device-side wait of the FP32 path gave up");
+  }
   return LB3DC_OK;
 }
 

@@ -1,0 +1,599 @@
+// fp32_mfield.cuh -- the moment-field strategy (strategy 3) of the FP32
+// deviation path, included by fp32_path.cu after fp32_split.cuh.
+//
+// Passes per step (binary lattices skip the second):
+//
+//   k_mf_moments: the pulls of every fluid site's 19*nc post-stream
+//       deviations (code/lb3d_advection.F90:109-151 with the half-way
+//       bounce-back of code/lb3d_bc_bounce.F90:53-90), read once from HBM,
+//       reduced to the site's moment entries and written to halo-padded
+//       moment fields:
+//         ternary  MF1 = {drho_r, drho_b, drho_s, P_x}
+//                  MF2 = {rho_b - rho_r, da}
+//                  plain MFp = {P_y, P_z}
+//         binary   MF1 = {drho_r, drho_b, P_x, P_y}, plain MFp = {P_z, 0}
+//       where P = sum_c amass_c omega_c j_c is the weighted momentum of
+//       code/lb3d_collision.F90:560-587 and da the advected dipole flux
+//       (code/lb3d_advection.F90:137-148).
+//   k_mf_dipole (ternary): the dipole relaxation (code/lb3d_collision.F90:
+//       296-403) of every site from MF2 with a one-site halo, written to the
+//       dipole state and to the halo-padded dipole field DD = {d, 0}.
+//   k_mf_collide: psi deviations on the tile plus a one-site halo from MF1,
+//       the Shan-Chen force (code/lb3d_force_shanchen.F90:127-330) from them
+//       and (ternary) DD, the body force and the velocities, and the
+//       populations of the next step.
+//
+// The padded fields carry two extra sites on each side in x and y; the
+// sites on an x or y boundary also write their periodic image into the
+// padding, so a tile plus its one-site halo is one dense box.  The dipole and
+// collide passes march a column tile in z and receive every plane of their
+// input fields as one TMA box per field (cp.async.bulk.tensor), two planes
+// ahead of use, on one mbarrier per ring slot, with one CTA barrier per plane.
+//
+// The populations are read once per step, by the moments pass: the collide
+// pass writes the equilibrium, which is the BGK update
+// (code/lb3d_collision.F90:258-284) when every component relaxes fully
+// (omega_c = 1, tau_c = 1: the populations' own values drop out); the
+// strategy is offered for such lattices only.  Every quantity is evaluated
+// with the expressions and in the order of the split strategies, so strategy
+// 3 equals them bit for bit (up to the sign of zero).
+//
+// The tensor maps cover this GPU's own moment field only and the loads do
+// not multicast.
+
+// ---- TMA and mbarrier primitives (PTX) -----------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n"
+      ".reg .pred p;\n"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on one phase of an mbarrier: false if it did not complete
+// within the iteration limit (each try_wait suspends for a bounded time).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+  for (int i = 0; i < (1 << 21); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// One 4-D tiled box global -> shared, completing on `bar` (no multicast).
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_desc(const void *tmap) {
+  asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
+}
+
+// Geometry shared by the passes: padded fields with MF_PAD extra sites on
+// each side in x and y (one of them used as the periodic image), ring boxes
+// of the tile plus a one-site halo.
+constexpr int MF_PAD = 2;
+template <int NC, int TX, int TY>
+struct MfGeom {
+  static constexpr int NT = TX * TY;
+  static constexpr int AW = TX + 2, AN = AW * (TY + 2);  // ring box, one-site halo
+  static constexpr int BOX_BYTES = 16 * AN;
+  // a TMA destination in shared memory starts on a 128-byte boundary: the
+  // boxes of one slot sit FIELD bytes apart
+  static constexpr int FIELD = (BOX_BYTES + 127) / 128 * 128;
+  // dipole pass: one MF2 box per slot, 5 slots
+  static constexpr int D_SLOT = (FIELD + 1023) / 1024 * 1024;
+  static constexpr int D_RS = 5;
+  static constexpr int D_SMEM = D_RS * D_SLOT + 1024;
+  // collide pass: MF1 (+ DD) boxes per slot, 6 slots; psi ring of 4 planes
+  static constexpr int NF = NC == 3 ? 2 : 1;
+  static constexpr int C_SLOT = (NF * FIELD + 1023) / 1024 * 1024;
+  static constexpr int C_RS = 6, PR = 4;
+  static constexpr int PSI_BYTES = PR * AN * (NC == 3 ? 16 : 8);
+  static constexpr int C_SMEM = C_RS * C_SLOT + PSI_BYTES + 1024;
+  static constexpr int AHEAD = 2;  // planes loaded ahead of use
+  static constexpr int C_MINB = NT >= 256 ? 2 : 3;
+};
+
+static_assert(MfGeom<3, 32, 8>::FIELD % 128 == 0 && MfGeom<3, 32, 8>::D_SLOT % 1024 == 0 &&
+                  MfGeom<3, 32, 8>::C_SLOT % 1024 == 0 && MfGeom<3, 32, 8>::C_SLOT >= 2 * MfGeom<3, 32, 8>::FIELD,
+              "TMA destinations of the ring slots must be 128-byte aligned");
+
+// Writes a float4 entry of site (gx, gy, gz) to a padded field, and its
+// periodic image when the site lies on an x or y boundary (nx, ny >= 2).
+__device__ __forceinline__ void mf_put(float4 *__restrict__ M, float4 e, int gx, int gy, int gz, int nx,
+                                       int ny) {
+  const int XP = nx + 2 * MF_PAD, YP = ny + 2 * MF_PAD;
+  const int xi = gx == 0 ? nx : (gx == nx - 1 ? -1 : gx);
+  const int yi = gy == 0 ? ny : (gy == ny - 1 ? -1 : gy);
+  const size_t zoff = (size_t)XP * YP * gz;
+  M[zoff + (gx + MF_PAD) + (size_t)XP * (gy + MF_PAD)] = e;
+  if (xi != gx) M[zoff + (xi + MF_PAD) + (size_t)XP * (gy + MF_PAD)] = e;
+  if (yi != gy) M[zoff + (gx + MF_PAD) + (size_t)XP * (yi + MF_PAD)] = e;
+  if (xi != gx && yi != gy) M[zoff + (xi + MF_PAD) + (size_t)XP * (yi + MF_PAD)] = e;
+}
+
+// ---------------------------------------------------------------------------
+// Moments pass: one thread per tile site, marching the tile's z range; the
+// previous dipoles (ternary) stream through a four-plane ring with a
+// one-site halo, refilled with cp.async one plane ahead, for the advected
+// flux.  Binary lattices need no ring and their threads never wait on each
+// other.
+// ---------------------------------------------------------------------------
+template <int NC, int TX, int TY, bool ROCK, bool NARROW>
+__global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
+    k_mf_moments(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
+                 const float *f0, const float *f1, const float *db0, const float *db1,
+                 const uint8_t *__restrict__ rock, unsigned S, float4 *__restrict__ MF1,
+                 float4 *__restrict__ MF2, float2 *__restrict__ MFp) {
+  constexpr int NT = TX * TY, DW = TX + 2, DN = DW * (TY + 2), DR = 4;
+  extern __shared__ float4 smd[];  // previous dipoles [DR][DN] (ternary)
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    const LatDesc &Lg = lats[T.lat];
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    const int par = Lg.parity;
+    const float *__restrict__ F = par ? f1 : f0;
+    const float *__restrict__ DBi = (NC == 3) ? (par ? db1 : db0) : nullptr;
+    const float rho0 = Lg.rho0;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool act = gx < nx && gy < ny;
+    // the ring of previous dipoles: plane z0 - 1 + j in slot j % DR
+    auto load_db_plane = [&](int j) {
+      const int gz = wrapz(z0 - 1 + j, nz);
+      float *dst = reinterpret_cast<float *>(smd + (j % DR) * DN);
+      for (int s = tid; s < DN; s += NT) {
+        const int ix = wrapz(x0 - 1 + s % DW, nx), iy = wrapz(y0 - 1 + s / DW, ny);
+        const int i = ix + nx * (iy + ny * gz);
+        cp_async4(dst + 4 * s, DBi + i);
+        cp_async4(dst + 4 * s + 1, DBi + S + i);
+        cp_async4(dst + 4 * s + 2, DBi + 2 * S + i);
+      }
+    };
+    if (NC == 3) {
+      load_db_plane(0);
+      load_db_plane(1);
+      load_db_plane(2);
+      cp_async_commit();
+    }
+    for (int it = 0; it < zc; ++it) {
+      if (NC == 3) {
+        if (it + 3 <= zc + 1) load_db_plane(it + 3);
+        cp_async_commit();
+        cp_async_wait<1>();  // planes up to it + 2 landed (this thread's copies)
+        __syncthreads();     // ... and everybody's
+      }
+      bool fluid = act;
+      Nbr nb;
+      int self = 0, gz = 0;
+      if (act) {
+        gz = wrapz(z0 + it, nz);
+        make_nbr(nb, gx, gy, gz, nx, ny, nz);
+        self = noff<18, 1>(nb);
+        // rock sites are never collided and their entries are never read
+        // (the force stencil takes the rock colour there): no pulls
+        if (ROCK) fluid = __ldg(rock + self) == 0;
+      }
+      if (fluid) {
+        float dr[NC], jm[NC][3];
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+        const float4 *Dm = smd + (it % DR) * DN, *D0 = smd + ((it + 1) % DR) * DN,
+                     *Dp = smd + ((it + 2) % DR) * DN;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          float d[19];
+          pull_comp<ROCK, false, NARROW>(F, S, c, nb, self, rock, d);
+          own_moments<1>(d, dr[c], jm[c][0], jm[c][1], jm[c][2]);
+          if (NC == 3 && c == 2) {
+            // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
+            const int ds0 = (tx + 1) + DW * (ty + 1);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+              const float4 *Dq = cz(q) == 1 ? Dm : (cz(q) == -1 ? Dp : D0);
+              const float4 b = Dq[ds0 - cx(q) - DW * cy(q)];
+              const float ng = (float)gw(q) * fmaf(wq(q), rho0, d[q]);
+              a0 = fmaf(ng, b.x, a0);
+              a1 = fmaf(ng, b.y, a1);
+              a2 = fmaf(ng, b.z, a2);
+            }
+          }
+        }
+        // the weighted momentum of the common velocity, summed as the
+        // collide passes sum it
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float am = Lg.amass[c] * Lg.omega[c];
+          p0 = fmaf(am, jm[c][0], p0);
+          p1 = fmaf(am, jm[c][1], p1);
+          p2 = fmaf(am, jm[c][2], p2);
+        }
+        if (NC == 3) {
+          MFp[self] = make_float2(p1, p2);
+          mf_put(MF1, make_float4(dr[0], dr[1], dr[NC - 1], p0), gx, gy, gz, nx, ny);
+          mf_put(MF2, make_float4(dr[1] - dr[0], a0, a1, a2), gx, gy, gz, nx, ny);
+        } else {
+          MFp[self] = make_float2(p2, 0.0f);
+          mf_put(MF1, make_float4(dr[0], dr[1], p0, p1), gx, gy, gz, nx, ny);
+        }
+      }
+      if (NC == 3) __syncthreads();  // the next iteration refills a ring slot read here
+    }
+    if (NC == 3) cp_async_wait<0>();
+  }
+}
+
+// Issues the TMA boxes of one plane into a ring slot (1024-byte aligned):
+// one or two float4 fields of the tile plus a one-site halo, at padded
+// coordinates (x0 + 1, y0 + 1), the second box `field` bytes (a multiple of
+// 128) after the first, on the slot's mbarrier.
+__device__ __forceinline__ void mf_issue(unsigned char *slot, int box_bytes, int field, const CUtensorMap *ma,
+                                         const CUtensorMap *mb, int x0, int y0, int zw, uint64_t *bar) {
+  mbar_expect_tx(bar, (mb ? 2 : 1) * box_bytes);
+  tma_load_4d(slot, ma, 0, x0 + MF_PAD - 1, y0 + MF_PAD - 1, zw, bar);
+  if (mb) tma_load_4d(slot + field, mb, 0, x0 + MF_PAD - 1, y0 + MF_PAD - 1, zw, bar);
+}
+
+// 1024-byte aligned start of the dynamic shared memory (TMA destinations).
+__device__ __forceinline__ unsigned char *mf_smem_base(unsigned char *raw) {
+  return reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(raw) + 1023) &
+                                           ~static_cast<uintptr_t>(1023));
+}
+
+// ---------------------------------------------------------------------------
+// Dipole pass (ternary).  Plane m of a tile is moment-field plane z0 - 1 + m
+// (m = 0 .. zc + 1); iteration j waits for plane j of MF2 and relaxes the
+// dipoles of plane j - 1 on the tile, dipole_site's arithmetic on the
+// {rho_b - rho_r, da} entries as the split strategies run it.  *err receives
+// LB3DC_ETIMEOUT if a plane never arrives.
+// ---------------------------------------------------------------------------
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
+    k_mf_dipole(const __grid_constant__ CUtensorMap tm2, const LatDesc *__restrict__ lats,
+                const Tile *__restrict__ tiles, int ntiles, float *db0, float *db1,
+                const float4 *__restrict__ MF1, float4 *__restrict__ DD, int *err) {
+  using G = MfGeom<3, TX, TY>;
+  constexpr int AW = G::AW, RS = G::D_RS, AHEAD = G::AHEAD;
+  extern __shared__ unsigned char smraw_[];
+  unsigned char *ring = mf_smem_base(smraw_);
+  __shared__ __align__(8) uint64_t bars[RS];
+  __shared__ LatDesc sLat;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  if (tid == 0) {
+    for (int s = 0; s < RS; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    tma_prefetch_desc(&tm2);
+  }
+  __syncthreads();
+  auto box = [&](unsigned g) { return reinterpret_cast<const float4 *>(ring + (g % RS) * G::D_SLOT); };
+  unsigned gbase = 0, issued = 0, waited = 0;
+  bool failed = false;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    if (tid == 0) sLat = lats[T.lat];
+    __syncthreads();
+    const LatDesc &Lg = sLat;
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    float *__restrict__ DBo = Lg.parity ? db0 : db1;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const int npl = zc + 2;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool act = gx < nx && gy < ny;
+    auto issue = [&](int m) {
+      const unsigned g = gbase + (unsigned)m;
+      mf_issue(ring + (g % RS) * G::D_SLOT, G::BOX_BYTES, G::FIELD, &tm2, nullptr, x0, y0,
+               wrapz(z0 - 1 + m, nz), &bars[g % RS]);
+    };
+    if (tid == 0)
+      for (int m = 0; m < AHEAD && m < npl; ++m) issue(m);
+    issued = gbase + (unsigned)(AHEAD < npl ? AHEAD : npl);
+    for (int j = 0; j < npl; ++j) {
+      const unsigned g = gbase + (unsigned)j;
+      const bool ok = mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
+      // every thread is past iteration j - 1, which last read the slot
+      // refilled below, and plane j has landed
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        waited = g;
+        break;
+      }
+      if (j + AHEAD < npl) {
+        if (tid == 0) issue(j + AHEAD);
+        issued = g + AHEAD + 1;
+      }
+      if (j >= 2 && act) {
+        const int as = (tx + 1) + AW * (ty + 1);
+        const int gz = wrapz(z0 + j - 2, nz);
+        const int XP = nx + 2 * MF_PAD, YP = ny + 2 * MF_PAD;
+        // the site's own surfactant density deviation
+        const float drs =
+            __ldg(MF1 + (size_t)XP * YP * gz + (gx + MF_PAD) + (size_t)XP * (gy + MF_PAD)).z;
+        const float3 d = dipole_site<AW>(box(g - 2), box(g - 1), box(g), as, Lg, Lg.rho0, drs);
+        const int i = gx + nx * (gy + ny * gz);
+        __stcs(DBo + i, d.x);
+        __stcs(DBo + (size_t)Lg.nx * Lg.ny * Lg.nz + i, d.y);
+        __stcs(DBo + 2 * (size_t)Lg.nx * Lg.ny * Lg.nz + i, d.z);
+        mf_put(DD, make_float4(d.x, d.y, d.z, 0.0f), gx, gy, gz, nx, ny);
+      }
+    }
+    if (failed) break;
+    gbase += (unsigned)npl;
+    __syncthreads();  // sLat and the ring are reused by the next tile
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicExch(err, LB3DC_ETIMEOUT);
+      for (unsigned g = waited; g < issued; ++g) mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
+    }
+    __syncthreads();
+  }
+}
+
+// Equilibrium deviations of one component written straight to the output
+// (full relaxation: the BGK update with omega = 1), with bgk_update's
+// arithmetic; out[q * S] receives population q.
+__device__ __forceinline__ void eq_store(float *out, unsigned S, float rho, float drho, float vx, float vy,
+                                         float vz, float omega) {
+  const float tx = 3.0f * vx, ty = 3.0f * vy, tz = 3.0f * vz;
+  const float uke = 0.5f * fmaf(tz, vz, fmaf(ty, vy, tx * vx));
+  const float a = -uke;
+  const float b = 1.0f + a;
+  const float orw = (omega * rho) * W1;
+  const float obase = (omega * drho) * W1;
+#define LB3D_EQ32(CD, I, J)                                               \
+  {                                                                       \
+    const float e = (CD);                                                 \
+    const float e2 = e * e;                                               \
+    const float ev = fmaf(orw, fmaf(0.5f, e2, a), obase);                 \
+    const float od = (orw * e) * fmaf(e2, 1.0f / 6.0f, b);                \
+    __stcs(out + (I) * S, ev + od);                                       \
+    __stcs(out + (J) * S, ev - od);                                       \
+  }
+  LB3D_EQ32(tx, 0, 1)
+  LB3D_EQ32(ty, 2, 3)
+  LB3D_EQ32(tz, 4, 5)
+  LB3D_EQ32(tx + ty, 6, 11)
+  LB3D_EQ32(tx - ty, 7, 10)
+  LB3D_EQ32(tx + tz, 8, 13)
+  LB3D_EQ32(tx - tz, 9, 12)
+  LB3D_EQ32(ty + tz, 14, 17)
+  LB3D_EQ32(ty - tz, 15, 16)
+#undef LB3D_EQ32
+  __stcs(out + 18 * S, fmaf((omega * rho) * W0, a, (omega * drho) * W0));
+}
+// eq_store for two components (lanes x, y) with bgk_update2's paired
+// arithmetic; lane x goes to outA, lane y to outB.
+__device__ __forceinline__ void eq_store2(float *outA, float *outB, unsigned S, float2 rho, float2 drho,
+                                          float2 vx, float2 vy, float2 vz, float2 omega) {
+  const float2 tx = mul2(f2(3.0f), vx), ty = mul2(f2(3.0f), vy), tz = mul2(f2(3.0f), vz);
+  const float2 uke = mul2(f2(0.5f), fma2(tz, vz, fma2(ty, vy, mul2(tx, vx))));
+  const float2 a = neg2(uke);
+  const float2 b = add2(f2(1.0f), a);
+  const float2 orw = mul2(mul2(omega, rho), f2(W1));
+  const float2 obase = mul2(mul2(omega, drho), f2(W1));
+#define LB3D_EQ2(CD, I, J)                                                    \
+  {                                                                           \
+    const float2 e = (CD);                                                    \
+    const float2 e2 = mul2(e, e);                                             \
+    const float2 ev = fma2(orw, fma2(f2(0.5f), e2, a), obase);                \
+    const float2 od = mul2(mul2(orw, e), fma2(e2, f2(1.0f / 6.0f), b));       \
+    const float2 p = add2(ev, od), m = add2(ev, neg2(od));                    \
+    __stcs(outA + (I) * S, p.x);                                              \
+    __stcs(outB + (I) * S, p.y);                                              \
+    __stcs(outA + (J) * S, m.x);                                              \
+    __stcs(outB + (J) * S, m.y);                                              \
+  }
+  LB3D_EQ2(tx, 0, 1)
+  LB3D_EQ2(ty, 2, 3)
+  LB3D_EQ2(tz, 4, 5)
+  LB3D_EQ2(add2(tx, ty), 6, 11)
+  LB3D_EQ2(add2(tx, neg2(ty)), 7, 10)
+  LB3D_EQ2(add2(tx, tz), 8, 13)
+  LB3D_EQ2(add2(tx, neg2(tz)), 9, 12)
+  LB3D_EQ2(add2(ty, tz), 14, 17)
+  LB3D_EQ2(add2(ty, neg2(tz)), 15, 16)
+#undef LB3D_EQ2
+  const float2 oeq0 = fma2(mul2(mul2(omega, rho), f2(W0)), a, mul2(mul2(omega, drho), f2(W0)));
+  __stcs(outA + 18 * S, oeq0.x);
+  __stcs(outB + 18 * S, oeq0.y);
+}
+
+// ---------------------------------------------------------------------------
+// Collide pass.  Plane m of a tile is field plane z0 - 1 + m (m = 0 ..
+// zc + 1).  Iteration j (0 .. zc + 2) waits for plane j, computes its psi
+// deviations on the tile plus a one-site halo into the psi ring, and the
+// force and equilibrium of plane j - 2 on the tile (whose psi planes were
+// computed in earlier iterations), so one CTA barrier per plane separates
+// the ring's writers from its readers.  *err receives LB3DC_ETIMEOUT if a
+// plane never arrives.
+// ---------------------------------------------------------------------------
+template <int NC, int TX, int TY, bool ROCK, bool BODY>
+__global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
+    k_mf_collide(const __grid_constant__ CUtensorMap tm1, const __grid_constant__ CUtensorMap tmd,
+                 const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles, float *f0,
+                 float *f1, const uint8_t *__restrict__ rock, unsigned S, const float2 *__restrict__ MFp,
+                 int *err) {
+  using G = MfGeom<NC, TX, TY>;
+  constexpr int AW = G::AW, AN = G::AN, RS = G::C_RS, PR = G::PR, AHEAD = G::AHEAD;
+  extern __shared__ unsigned char smraw_[];
+  unsigned char *ring = mf_smem_base(smraw_);
+  unsigned char *psiring = ring + RS * G::C_SLOT;
+  __shared__ __align__(8) uint64_t bars[RS];
+  __shared__ LatDesc sLat;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  constexpr int NT = G::NT;
+  if (tid == 0) {
+    for (int s = 0; s < RS; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    tma_prefetch_desc(&tm1);
+    if (NC == 3) tma_prefetch_desc(&tmd);
+  }
+  __syncthreads();
+  auto box = [&](unsigned g, int f) {
+    return reinterpret_cast<const float4 *>(ring + (g % RS) * G::C_SLOT + f * G::FIELD);
+  };
+  unsigned gbase = 0, issued = 0, waited = 0;
+  bool failed = false;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile T = tiles[t];
+    if (tid == 0) sLat = lats[T.lat];
+    __syncthreads();
+    const LatDesc &Lg = sLat;
+    const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
+    float *__restrict__ Fo = Lg.parity ? f0 : f1;
+    const float psi0 = Lg.psi0, em0 = Lg.em0;
+    const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
+    const int npl = zc + 2;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool act = gx < nx && gy < ny;
+    auto issue = [&](int m) {
+      const unsigned g = gbase + (unsigned)m;
+      mf_issue(ring + (g % RS) * G::C_SLOT, G::BOX_BYTES, G::FIELD, &tm1, NC == 3 ? &tmd : nullptr, x0,
+               y0, wrapz(z0 - 1 + m, nz), &bars[g % RS]);
+    };
+    if (tid == 0)
+      for (int m = 0; m < AHEAD && m < npl; ++m) issue(m);
+    issued = gbase + (unsigned)(AHEAD < npl ? AHEAD : npl);
+    for (int j = 0; j <= npl; ++j) {
+      const unsigned g = gbase + (unsigned)j;
+      bool ok = true;
+      if (j < npl) ok = mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
+      // every thread is past iteration j - 1 (the psi slot written below and
+      // the ring slot refilled below were last read there) and plane j landed
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        waited = g;
+        break;
+      }
+      if (j + AHEAD < npl) {
+        if (tid == 0) issue(j + AHEAD);
+        issued = g + AHEAD + 1;
+      }
+      // ---- psi deviations of plane j on the tile plus a one-site halo
+      if (j < npl) {
+        const float4 *M1 = box(g, 0);
+        for (int s = tid; s < AN; s += NT) {
+          const float4 e = M1[s];
+          if constexpr (NC == 3)
+            reinterpret_cast<float4 *>(psiring)[(j % PR) * AN + s] =
+                make_float4(0.0f, -em0 * expm1f(-e.x), -em0 * expm1f(-e.y), -em0 * expm1f(-e.z));
+          else
+            reinterpret_cast<float2 *>(psiring)[(j % PR) * AN + s] =
+                make_float2(-em0 * expm1f(-e.x), -em0 * expm1f(-e.y));
+        }
+      }
+      // ---- force and equilibrium of plane mc = j - 2 on the tile
+      const int mc = j - 2;
+      if (mc >= 1 && mc <= zc && act) {
+        const int gz = wrapz(z0 - 1 + mc, nz);
+        Nbr nb;
+        make_nbr(nb, gx, gy, gz, nx, ny, nz);
+        const int self = noff<18, 1>(nb);
+        bool own_rock = false;
+        if (ROCK) own_rock = __ldg(rock + self) != 0;
+        if (!own_rock) {
+          const int ap = (tx + 1) + AW * (ty + 1);
+          const unsigned gc = gbase + (unsigned)mc;
+          float Fx[NC][3];
+          if constexpr (NC == 3) {
+            const float4 *P4 = reinterpret_cast<const float4 *>(psiring);
+            force_ternary<AW, AW>(P4 + ((mc + PR - 1) % PR) * AN, P4 + (mc % PR) * AN,
+                                  P4 + ((mc + 1) % PR) * AN, DipF4{box(gc - 1, 1)}, DipF4{box(gc, 1)},
+                                  DipF4{box(gc + 1, 1)}, ap, ap, Lg, psi0,
+                                  reinterpret_cast<float(*)[3]>(Fx));
+          } else {
+            const float2 *P2 = reinterpret_cast<const float2 *>(psiring);
+            force_binary<AW, ROCK>(P2 + ((mc + PR - 1) % PR) * AN, P2 + (mc % PR) * AN,
+                                   P2 + ((mc + 1) % PR) * AN, ap, nb, rock, Lg, psi0,
+                                   reinterpret_cast<float(*)[3]>(Fx));
+          }
+          // own densities and weighted momentum
+          const float4 o1 = box(gc, 0)[ap];
+          const float2 op = __ldg(MFp + self);
+          float dr[NC], rho[NC], pp[3];
+          if constexpr (NC == 3) {
+            dr[0] = o1.x, dr[1] = o1.y, dr[NC - 1] = o1.z;
+            pp[0] = o1.w, pp[1] = op.x, pp[2] = op.y;
+          } else {
+            dr[0] = o1.x, dr[1] = o1.y;
+            pp[0] = o1.z, pp[1] = o1.w, pp[2] = op.x;
+          }
+#pragma unroll
+          for (int c = 0; c < NC; ++c) rho[c] = Lg.rho0 + dr[c];
+          if (BODY) {
+            const int x1 = gx + 1, y1 = gy + 1, z1 = gz + 1;
+            bool on;
+            if (Lg.inv_fluid == 9)
+              on = (z1 == 1) || (z1 == nz);
+            else if (Lg.inv_fluid == 20 || Lg.inv_fluid == 21)
+              on = z1 == 1;
+            else
+              on = z1 >= Lg.amin_z && z1 <= Lg.amax_z && x1 >= Lg.amin_x && x1 <= Lg.amax_x &&
+                   y1 >= Lg.amin_y && y1 <= Lg.amax_y;
+            if (on) {
+#pragma unroll
+              for (int c = 0; c < NC; ++c) {
+                const float m = Lg.amass[c] * rho[c];
+                Fx[c][0] = fmaf(m, Lg.g_accn_x, Fx[c][0]);
+                Fx[c][1] = fmaf(m, Lg.g_accn_y, Fx[c][1]);
+                Fx[c][2] = fmaf(m, Lg.g_accn, Fx[c][2]);
+              }
+            }
+          }
+          float rt = 0.f;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) rt = fmaf(Lg.amass[c] * Lg.omega[c], rho[c], rt);
+          const float irt = 1.0f / fmaxf(rt, 1.0e-8f);
+          const float u0 = pp[0] * irt, u1 = pp[1] * irt, u2 = pp[2] * irt;
+          float vx[NC], vy[NC], vz[NC];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const float kf = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
+            vx[c] = fmaf(kf, Fx[c][0], u0);
+            vy[c] = fmaf(kf, Fx[c][1], u1);
+            vz[c] = fmaf(kf, Fx[c][2], u2);
+          }
+          float *fo = Fo + self;
+          eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+                    make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
+                    make_float2(Lg.omega[0], Lg.omega[1]));
+          if (NC == 3)
+            eq_store(fo + (size_t)38 * S, S, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1],
+                     Lg.omega[NC - 1]);
+        }
+      }
+    }
+    if (failed) break;
+    gbase += (unsigned)npl;
+    __syncthreads();  // sLat and the rings are reused by the next tile
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicExch(err, LB3DC_ETIMEOUT);
+      for (unsigned g = waited; g < issued; ++g) mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
+    }
+    __syncthreads();
+  }
+}

@@ -661,6 +661,7 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
 }
 
 #include "fp32_split.cuh"
+#include "fp32_mfield.cuh"
 
 __global__ void k_flip(LatDesc *lats, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1045,9 +1046,249 @@ long long fp32_footprint(const lb3dc_params &p) {
   const long long N = (long long)p.nx * p.ny * p.nz;
   const bool le = p.boundary_cond != 0 && (p.inv_fluid == 5 || p.inv_fluid == 6);
   const long long np = (long long)p.ny * p.nz;
+  // the moment field of strategy 3 when every component relaxes fully
+  const bool full = p.tau_r == 1.0 && p.tau_b == 1.0 && (p.ncomp == 2 || p.tau_s == 1.0);
+  const long long mf = full && !le ? (long long)(p.nx + 2 * MF_PAD) * (p.ny + 2 * MF_PAD) * p.nz *
+                                             (p.ncomp == 3 ? 48 : 16) + N * 8
+                                   : 0;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
-         N * fp32_moment_bytes(p.ncomp) +
+         N * fp32_moment_bytes(p.ncomp) + mf +
          (le ? 2 * np * (p.ncomp * 19 * 4 + 8) : 0) + N * 8 + 4096;
+}
+
+// ---------------------------------------------------------------------------
+// moment-field strategy (split 3): eligibility, field, tensor maps, launches
+// ---------------------------------------------------------------------------
+bool fp32_mf_eligible(const DevParams &P) {
+  if (P.le || P.invk) return false;
+  for (int c = 0; c < P.nc; ++c)
+    if (P.omega[c] != 1.0) return false;
+  if (P.nx < 2 || P.ny < 2) return false;
+  return (long long)(P.nx + 2 * MF_PAD) * (P.ny + 2 * MF_PAD) * P.nz < (1LL << 31);
+}
+
+long long fp32_mf_bytes(const DevParams &P) {
+  return (long long)(P.nx + 2 * MF_PAD) * (P.ny + 2 * MF_PAD) * P.nz * (P.nc == 3 ? 48 : 16) +
+         P.nsites * 8 + 64;
+}
+
+static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
+  if (s.MF1) return LB3DC_OK;
+  const size_t plane = (size_t)(P.nx + 2 * MF_PAD) * (P.ny + 2 * MF_PAD) * P.nz * sizeof(float4);
+  bool ok = cudaMalloc(&s.MF1, plane) == cudaSuccess;
+  if (ok && P.nc == 3) ok = cudaMalloc(&s.MF2, plane) == cudaSuccess;
+  if (ok && P.nc == 3) ok = cudaMalloc(&s.DD, plane) == cudaSuccess;
+  if (ok) ok = cudaMalloc(&s.MFp, (size_t)P.nsites * sizeof(float2)) == cudaSuccess;
+  if (ok && !s.err) ok = cudaMalloc(&s.err, sizeof(int)) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    if (s.MF1) cudaFree(s.MF1);
+    if (s.MF2) cudaFree(s.MF2);
+    if (s.DD) cudaFree(s.DD);
+    if (s.MFp) cudaFree(s.MFp);
+    s.MF1 = s.MF2 = s.DD = nullptr;
+    s.MFp = nullptr;
+    return LB3DC_ENOMEM;
+  }
+  // padding entries that no site writes are read only by inactive lanes
+  cudaMemsetAsync(s.MF1, 0, plane, st);
+  if (s.MF2) cudaMemsetAsync(s.MF2, 0, plane, st);
+  if (s.DD) cudaMemsetAsync(s.DD, 0, plane, st);
+  cudaMemsetAsync(s.err, 0, sizeof(int), st);
+  s.bytes += (long long)plane * (P.nc == 3 ? 3 : 1) + P.nsites * 8;
+  return LB3DC_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// A padded float4 field as a 4-D FP32 tensor {component 0..3, padded x,
+// padded y, z}; one box is the tile plus one halo site in x and y, one plane
+// deep.
+static int encode_mf_map(CUtensorMap *m, float4 *base, const DevParams &P, int tx, int ty) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return LB3DC_ECUDA;
+  const cuuint64_t XP = (cuuint64_t)P.nx + 2 * MF_PAD, YP = (cuuint64_t)P.ny + 2 * MF_PAD;
+  const cuuint64_t dims[4] = {4, XP, YP, (cuuint64_t)P.nz};
+  const cuuint64_t strides[3] = {16, 16 * XP, 16 * XP * YP};
+  const cuuint32_t box[4] = {4, (cuuint32_t)(tx + 2), (cuuint32_t)(ty + 2), 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LB3DC_OK : LB3DC_ECUDA;
+}
+
+template <int NC, int TX, int TY, bool ROCK, bool BODY>
+static void mf_ptrs(bool narrow, const void **mom, const void **dip, const void **col) {
+  *mom = narrow ? (const void *)k_mf_moments<NC, TX, TY, ROCK, true>
+                : (const void *)k_mf_moments<NC, TX, TY, ROCK, false>;
+  *dip = NC == 3 ? (const void *)k_mf_dipole<TX, TY> : nullptr;
+  *col = (const void *)k_mf_collide<NC, TX, TY, ROCK, BODY>;
+}
+// The kernels of strategy 3 for a lattice kind and tile shape (false if the
+// shape is not compiled); dip is null for binary lattices.
+static bool mf_fns(int nc, bool rock, bool body, int tx, int ty, bool narrow, const void **mom,
+                   const void **dip, const void **col) {
+#define LB3D_MF(NC, R, B)                                                                \
+  if (tx == 32 && ty == 8) return mf_ptrs<NC, 32, 8, R, B>(narrow, mom, dip, col), true;   \
+  if (tx == 32 && ty == 4) return mf_ptrs<NC, 32, 4, R, B>(narrow, mom, dip, col), true;   \
+  if (tx == 16 && ty == 16) return mf_ptrs<NC, 16, 16, R, B>(narrow, mom, dip, col), true; \
+  if (tx == 16 && ty == 8) return mf_ptrs<NC, 16, 8, R, B>(narrow, mom, dip, col), true;   \
+  if (tx == 64 && ty == 4) return mf_ptrs<NC, 64, 4, R, B>(narrow, mom, dip, col), true;
+  if (nc == 3) {
+    if (rock) return false;
+    if (body) { LB3D_MF(3, false, true) } else { LB3D_MF(3, false, false) }
+  } else if (rock) {
+    if (body) { LB3D_MF(2, true, true) } else { LB3D_MF(2, true, false) }
+  } else {
+    if (body) { LB3D_MF(2, false, true) } else { LB3D_MF(2, false, false) }
+  }
+#undef LB3D_MF
+  return false;
+}
+// Dynamic shared memory of pass `which` (0 moments, 1 dipole, 2 collide);
+// mirrors MfGeom.
+static size_t mf_smem(int nc, int tx, int ty, int which) {
+  const size_t an = (size_t)(tx + 2) * (ty + 2), field = (16 * an + 127) / 128 * 128;
+  if (which == 0) return nc == 3 ? 4 * an * 16 : 0;
+  if (which == 1) return 5 * ((field + 1023) / 1024 * 1024) + 1024;
+  const size_t slot = ((nc == 3 ? 2 : 1) * field + 1023) / 1024 * 1024;
+  return 6 * slot + 4 * an * (nc == 3 ? 16 : 8) + 1024;
+}
+
+// One step of strategy 3: the moments pass, (ternary) the dipole pass and the
+// collide pass, each on its own tile list and resident grid.
+static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *rockp, cudaStream_t st) {
+  const bool rock = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
+  const unsigned S = (unsigned)s.S;
+  const bool narrow = 19ull * P.nc * s.S < (1ull << 32);
+  const void *fn[3] = {nullptr, nullptr, nullptr};
+  if (!mf_fns(P.nc, rock, body, s.tx, s.ty, narrow, &fn[0], &fn[1], &fn[2]))
+    return cudaErrorInvalidConfiguration;
+  if (s.mf_tx != s.tx || s.mf_ty != s.ty || !s.mf_tiles) return cudaErrorInvalidConfiguration;
+  const int nt = s.tx * s.ty;
+  const LatDesc *dl = s.d_lat;
+  cudaError_t e = cudaSuccess;
+  for (int pass = 0; pass < 3 && e == cudaSuccess; ++pass) {
+    if (!fn[pass]) continue;
+    const size_t sm = mf_smem(P.nc, s.tx, s.ty, pass);
+    int res = 0;
+    if ((e = prepare_kernel(fn[pass], nt, sm, &res)) != cudaSuccess) break;
+    const Tile *dt = s.mf_tiles + s.mf_off[pass];
+    int ntl = s.mf_ntiles[pass];
+    const dim3 grid(std::max(1, std::min(ntl, res)));
+    if (pass == 0) {
+      const float *f0 = s.f[0], *f1 = s.f[1], *d0 = s.db[0], *d1 = s.db[1];
+      void *args[] = {(void *)&dl, (void *)&dt, (void *)&ntl, (void *)&f0, (void *)&f1, (void *)&d0,
+                      (void *)&d1, (void *)&rockp, (void *)&S, (void *)&s.MF1, (void *)&s.MF2,
+                      (void *)&s.MFp};
+      e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
+    } else if (pass == 1) {
+      const float4 *mf1 = s.MF1;
+      void *args[] = {(void *)&s.tm2, (void *)&dl, (void *)&dt, (void *)&ntl, (void *)&s.db[0],
+                      (void *)&s.db[1], (void *)&mf1, (void *)&s.DD, (void *)&s.err};
+      e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
+    } else {
+      const float2 *mfp = s.MFp;
+      void *args[] = {(void *)&s.tm1, (void *)&s.tmd, (void *)&dl, (void *)&dt, (void *)&ntl,
+                      (void *)&s.f[0], (void *)&s.f[1], (void *)&rockp, (void *)&S, (void *)&mfp,
+                      (void *)&s.err};
+      e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
+    }
+  }
+  return e;
+}
+
+// The z chunking of one pass of strategy 3: nxy column tiles, `resident`
+// CTAs at once, `halo` planes each chunk reads beyond its own.  Chooses the
+// number of chunks per column so that the tiles fill whole rounds of the
+// resident grid (1 to 8 rounds), weighed against the halo planes that
+// shorter chunks reload; the chunks of a column differ in length by at most
+// one plane.
+static int mf_chunks(int nz, int nxy, int resident, int halo) {
+  int best = 1;
+  double best_score = -1.0;
+  for (int rounds = 1; rounds <= 8; ++rounds) {
+    int k = std::min(nz, std::max(1, (int)((long long)rounds * resident / nxy)));
+    const long long nt = (long long)nxy * k;
+    const long long used = (nt + resident - 1) / resident * resident;
+    const double zc = (double)nz / k;
+    const double score = (double)nt / used * zc / (zc + halo);
+    if (score > best_score + 1e-9) best_score = score, best = k;
+  }
+  return best;
+}
+
+static int mf_build_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
+  const void *fn[3];
+  if (!mf_fns(P.nc, (s.lat.flags & LAT_ROCK) != 0, (s.lat.flags & LAT_BODY) != 0, sh.tx, sh.ty,
+              19ull * P.nc * s.S < (1ull << 32), &fn[0], &fn[1], &fn[2]))
+    return LB3DC_EINVAL;
+  const LatDesc &L = s.lat;
+  const int nxt = (L.nx + sh.tx - 1) / sh.tx, nyt = (L.ny + sh.ty - 1) / sh.ty, nxy = nxt * nyt;
+  std::vector<Tile> all;
+  // planes a chunk reads beyond its own: the dipole and collide passes load
+  // one field plane on each side; the moments pass counts one for the
+  // dipole planes its ring loads ahead of its first plane
+  const int halo[3] = {1, 2, 2};
+  for (int pass = 0; pass < 3; ++pass) {
+    s.mf_off[pass] = (int)all.size();
+    s.mf_ntiles[pass] = 0;
+    if (!fn[pass]) continue;
+    int res = 0;
+    if (prepare_kernel(fn[pass], sh.tx * sh.ty, mf_smem(P.nc, sh.tx, sh.ty, pass), &res) != cudaSuccess)
+      return LB3DC_ECUDA;
+    const int k = mf_chunks(L.nz, nxy, res, halo[pass]);
+    for (int c = 0; c < k; ++c) {
+      const int z0 = (int)((long long)L.nz * c / k), z1 = (int)((long long)L.nz * (c + 1) / k);
+      for (int y0 = 0; y0 < L.ny; y0 += sh.ty)
+        for (int x0 = 0; x0 < L.nx; x0 += sh.tx) {
+          Tile t;
+          t.lat = 0;
+          t.x0 = (short)x0;
+          t.y0 = (short)y0;
+          t.z0 = (short)z0;
+          t.zc = (short)(z1 - z0);
+          all.push_back(t);
+        }
+    }
+    s.mf_ntiles[pass] = (int)all.size() - s.mf_off[pass];
+    s.mf_grid[pass] = std::min(s.mf_ntiles[pass], res);
+  }
+  if (s.mf_tiles) cudaFree(s.mf_tiles);
+  s.mf_tiles = nullptr;
+  if (cudaMalloc(&s.mf_tiles, all.size() * sizeof(Tile)) != cudaSuccess) return LB3DC_ENOMEM;
+  if (cudaMemcpyAsync(s.mf_tiles, all.data(), all.size() * sizeof(Tile), cudaMemcpyHostToDevice, st) !=
+      cudaSuccess)
+    return LB3DC_ECUDA;
+  return cudaStreamSynchronize(st) == cudaSuccess ? LB3DC_OK : LB3DC_ECUDA;
+}
+
+int fp32_take_error(Fp32State &s, cudaStream_t st) {
+  if (!s.err) return LB3DC_OK;
+  int v = 0;
+  if (cudaMemcpyAsync(&v, s.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return LB3DC_ECUDA;
+  if (v) cudaMemsetAsync(s.err, 0, sizeof(int), st);
+  return v;
 }
 
 // The Lees-Edwards halo planes of a single lattice, referenced by its descriptor.
@@ -1086,6 +1327,28 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
     int rc = ensure_own(P, s);
     if (rc) return rc;
   }
+  if (sh.split == 3) {
+    if (!fp32_mf_eligible(P)) return LB3DC_ENOTSUP;
+    const void *a, *b, *c;
+    if (!mf_fns(P.nc, (s.lat.flags & LAT_ROCK) != 0, (s.lat.flags & LAT_BODY) != 0, sh.tx, sh.ty, true,
+                &a, &b, &c))
+      return LB3DC_EINVAL;
+    int rc = ensure_mf(P, s, st);
+    if (rc) return rc;
+    if (s.mf_tx != sh.tx || s.mf_ty != sh.ty) {
+      s.mf_tx = s.mf_ty = 0;
+      if ((rc = encode_mf_map(&s.tm1, s.MF1, P, sh.tx, sh.ty)) != LB3DC_OK) return rc;
+      if (P.nc == 3) {
+        if ((rc = encode_mf_map(&s.tm2, s.MF2, P, sh.tx, sh.ty)) != LB3DC_OK) return rc;
+        if ((rc = encode_mf_map(&s.tmd, s.DD, P, sh.tx, sh.ty)) != LB3DC_OK) return rc;
+      } else {
+        s.tm2 = s.tmd = s.tm1;  // unused by the binary kernels
+      }
+      s.mf_tx = sh.tx;
+      s.mf_ty = sh.ty;
+    }
+    if ((rc = mf_build_tiles(P, s, sh, st)) != LB3DC_OK) return rc;
+  }
   std::vector<Tile> tiles;
   fp32_tiles_for(s.lat, 0, sh, tiles);
   if (s.d_tiles) cudaFree(s.d_tiles);
@@ -1103,6 +1366,10 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   bool rock = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
+  if (sh.split == 3) {
+    s.grid = s.ntiles;  // each pass sizes its own grid at launch
+    return LB3DC_OK;
+  }
   int per = fp32_fused_ctas_per_sm(P.nc, rock, body, sh);
   if (per < 1) return LB3DC_EINVAL;
   s.grid = std::min(s.ntiles, per * nsm);
@@ -1114,8 +1381,9 @@ int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaS
   // Lees-Edwards lattices and lattices with inflow boundaries run the
   // staged split strategy only
   if ((s.le_h[0] || s.lat.invk) && sh.split != 2) return LB3DC_ENOTSUP;
+  if (sh.split == 3 && !fp32_mf_eligible(P)) return LB3DC_ENOTSUP;
   if (sh.split && !s.M) return LB3DC_EINVAL;
-  if (sh.split < 0 || sh.split > 2) return LB3DC_EINVAL;
+  if (sh.split < 0 || sh.split > 3) return LB3DC_EINVAL;
   if (sh.zc < 1) return LB3DC_EINVAL;
   return rebuild_tiles(P, s, sh, st);
 }
@@ -1130,6 +1398,14 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P) {
       if (zc > P.nz && zc != 8) continue;
       for (int split = (P.le || P.invk) ? 2 : 0; split < 3; ++split)
         out.push_back(FusedShape{t[0], t[1], zc, split});
+    }
+  }
+  // strategy 3 chunks z per pass from each pass's resident grid: one
+  // candidate per tile shape (its zc is not used)
+  if (fp32_mf_eligible(P)) {
+    for (auto &t : xy) {
+      if (t[0] > 2 * P.nx && t[0] > 16) continue;
+      out.push_back(FusedShape{t[0], t[1], 16, 3});
     }
   }
   return out;
@@ -1230,6 +1506,17 @@ void fp32_free(Fp32State &s) {
   if (s.d_tiles) cudaFree(s.d_tiles);
   if (s.M) cudaFree(s.M);
   if (s.J) cudaFree(s.J);
+  if (s.MF1) cudaFree(s.MF1);
+  if (s.MF2) cudaFree(s.MF2);
+  if (s.DD) cudaFree(s.DD);
+  if (s.MFp) cudaFree(s.MFp);
+  if (s.err) cudaFree(s.err);
+  if (s.mf_tiles) cudaFree(s.mf_tiles);
+  s.MF1 = s.MF2 = s.DD = nullptr;
+  s.MFp = nullptr;
+  s.mf_tiles = nullptr;
+  s.err = nullptr;
+  s.mf_tx = s.mf_ty = 0;
   if (s.stage) cudaFree(s.stage);
   s.stage = nullptr;
   for (int b = 0; b < 2; ++b) {
@@ -1368,11 +1655,14 @@ int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, 
   // kernels per step: the pass(es), two Lees-Edwards halo kernels, the parity flip
   const int passes = sh.split ? (P.nc == 3 ? 3 : 2) : 1;
   const int per_step = passes + (le ? 2 : 0) + 1;
+  if (sh.split == 3 && le) return LB3DC_ENOTSUP;
   for (int i = 0; i < nsteps; ++i) {
     if (s.timer) s.timer->start(st);
-    cudaError_t e = fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, 0,
-                                      s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M, s.J,
-                                      le, &P);
+    cudaError_t e = sh.split == 3
+                        ? launch_mf(P, s, rock, st)
+                        : fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, 0,
+                                            s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M,
+                                            s.J, le, &P);
     if (s.timer) {
       s.timer->stop(st);
       s.timer->launches += per_step;

@@ -5,6 +5,8 @@
 
 #include <vector>
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "reduce.h"
 
@@ -64,13 +66,29 @@ struct Fp32State {
   double *stage = nullptr;  // one FP64 population plane (N sites) for uploads and downloads
   float *le_h[2] = {nullptr, nullptr};  // Lees-Edwards halo planes (see LatDesc)
   float2 *le_p[2] = {nullptr, nullptr};
+  // moment-field strategy (split 3): the halo-padded moment fields (and
+  // dipole field, ternary), the plain momentum plane, the tensor maps of their
+  // TMA boxes (encoded for the tile shape mf_tx x mf_ty) and the device flag
+  // of a wait that gave up
+  float4 *MF1 = nullptr, *MF2 = nullptr, *DD = nullptr;
+  float2 *MFp = nullptr;
+  int *err = nullptr;
+  CUtensorMap tm1{}, tm2{}, tmd{};
+  int mf_tx = 0, mf_ty = 0;
+  // its tile lists, one per pass (moments, dipole, collide), each chunking z
+  // so that the tiles fill the pass's resident grid: mf_ntiles[p] tiles at
+  // mf_tiles + mf_off[p], launched on mf_grid[p] CTAs
+  Tile *mf_tiles = nullptr;
+  int mf_ntiles[3] = {0, 0, 0}, mf_off[3] = {0, 0, 0}, mf_grid[3] = {0, 0, 0};
 };
 
 // Launch configuration of the fused kernel.
 struct FusedShape {
   int tx, ty, zc;
   int split = 0;  // 0: one fused pass per step; 1: moments (+ dipole) + collide passes;
-                  // 2: as 1 with the asynchronously staged collide pass (no J field)
+                  // 2: as 1 with the asynchronously staged collide pass (no J field);
+                  // 3: moment field + TMA-fed dipole/force/equilibrium pass (full
+                  //    relaxation only, single lattices)
 };
 
 long long fp32_footprint(const lb3dc_params &p);
@@ -136,6 +154,15 @@ std::vector<FusedShape> fp32_candidate_shapes(const DevParams &P);
 int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double *ms_out,
                   int *ntried, cudaStream_t st, const LEStep *le = nullptr);
 int fp32_fused_ctas_per_sm(int nc, bool rock, bool body, const FusedShape &sh);
+// The moment-field strategy applies: every component relaxes fully
+// (omega = 1), periodic or walled lattice without Lees-Edwards planes or
+// inflow boundaries, at least 2 sites across in x and y.
+bool fp32_mf_eligible(const DevParams &P);
+// Bytes of the moment and dipole fields of strategy 3.
+long long fp32_mf_bytes(const DevParams &P);
+// The device error flag of the handle's kernels (0, or LB3DC_ETIMEOUT when a
+// bounded wait gave up), read and cleared; LB3DC_OK when no flag exists.
+int fp32_take_error(Fp32State &s, cudaStream_t st);
 
 }  // namespace lb3d
 #endif

@@ -10,9 +10,11 @@
 // is summed over the nine pairs of opposite neighbours (q, bounce(q)), whose
 // c_q terms differ only in sign: per pair the difference of phi and the sum
 // of da enter once.
-template <int AW>
-__device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0, const float4 *Ap,
-                                              int as, const LatDesc &Lg, float rho0, float own_drs) {
+// AP is a pointer to the entries or an accessor with operator[] (the
+// moment-field strategy forms the entries from two ring boxes).
+template <int AW, typename AP>
+__device__ __forceinline__ float3 dipole_site(AP Am, AP A0, AP Ap, int as, const LatDesc &Lg, float rho0,
+                                              float own_drs) {
   const float4 own0 = A0[as];
   float P0 = 0.f, P1 = 0.f, P2 = 0.f;  // sum g c (phi_q - phi_qbar)
   float S0 = 0.f, S1 = 0.f, S2 = 0.f;  // sum g (da_q + da_qbar)
@@ -22,8 +24,8 @@ __device__ __forceinline__ float3 dipole_site(const float4 *Am, const float4 *A0
   for (int q = 0; q < 18; ++q) {
     if (bounce(q) < q) continue;  // each pair once, from its first member
     const int qb = bounce(q);
-    const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
-    const float4 *Ab = cz(qb) == 1 ? Ap : (cz(qb) == -1 ? Am : A0);
+    const AP &Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
+    const AP &Ab = cz(qb) == 1 ? Ap : (cz(qb) == -1 ? Am : A0);
     const float4 e = Aq[as + cx(q) + AW * cy(q)];
     const float4 f = Ab[as + cx(qb) + AW * cy(qb)];
     const float g = (float)gw(q);

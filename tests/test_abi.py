@@ -56,7 +56,9 @@ def test_footprint():
     fb = L.footprint(p)
     assert fb >= 2 * 3 * 19 * N * 8
     p.precision = 1
-    assert L.footprint(p) < fb / 1.9
+    # half the population bytes, plus the moment-field strategy's padded
+    # fields (48 B per site) when every component relaxes fully
+    assert L.footprint(p) < fb / 1.7
 
 
 @pytest.mark.parametrize("case", ["gyroid", "wettingWall"])

@@ -243,3 +243,80 @@ def test_fp32_inflow_runs_the_staged_split_strategy_only():
     lat.set_launch_shape(16, 8, 8, 2)
     lat.autotune()
     assert lat.launch_shape[3] == 2
+
+
+@pytest.mark.parametrize("nc,dims,shape,rock", [
+    (3, (40, 24, 20), (32, 8, 16), False),
+    (3, (7, 5, 6), (16, 8, 16), False),
+    (3, (4, 4, 3), (16, 8, 16), False),
+    (3, (33, 9, 40), (32, 4, 16), False),
+    (3, (70, 20, 12), (64, 4, 32), False),
+    (3, (36, 40, 24), (16, 16, 64), False),
+    (2, (40, 12, 33), (16, 16, 16), True),
+    (2, (9, 6, 5), (32, 4, 16), True),
+    (2, (2, 3, 4), (16, 8, 16), False),
+    (2, (64, 24, 20), (32, 8, 32), False),
+])
+def test_moment_field_strategy_equals_staged_split(nc, dims, shape, rock):
+    """Strategy 3 (moment field written by the moments pass, read back as TMA
+    boxes with a halo by the dipole/force/equilibrium pass) evaluates every
+    quantity as strategy 2 does, so with full relaxation (tau = 1) both give
+    the same bits: partial tiles, lattices narrower than a tile or than the
+    box halo, short z chunks, body force in a sub-box and bounce-back walls."""
+    from lb3d_b200.lib import Lattice
+    kw = dict(g_accn=1e-4, g_accn_min=2, g_accn_max=4, g_accn_x=-2e-5)
+    if rock:
+        kw.update(g_wr=-0.1, g_wb=0.05, rock_colour_r=1.0, rock_colour_b=0.5)
+    p = _params(dims, nc, **kw)
+    st = uniform_mixture(*dims, nc, seed=23)
+    if rock:
+        rng = np.random.default_rng(6)
+        st["rock"] = (rng.random(st["n"].shape[2:]) < 0.2).astype(np.float64)
+    out = []
+    for split in (2, 3):
+        lat = Lattice(p, precision=1)
+        lat.upload_state(st)
+        lat.set_launch_shape(*shape, split)
+        assert lat.launch_shape == (*shape, split)
+        lat.time_loop(25)
+        lat.sync()
+        out.append(lat.download())
+    assert np.array_equal(out[0]["n"], out[1]["n"])
+    if nc == 3:
+        assert np.array_equal(out[0]["db"], out[1]["db"])
+
+
+def test_moment_field_strategy_against_oracle():
+    """Strategy 3 on the gyroid reference system, against the FP64 oracle
+    within the FP32 tolerances."""
+    from lb3d_b200.lib import Lattice
+    p, st = load_case("gyroid")
+    lat = Lattice(p, precision=1)
+    lat.upload_state(st)
+    lat.set_launch_shape(16, 8, 16, 3)
+    lat.time_loop(20)
+    o = Oracle(p, st)
+    o.run(20)
+    check(lat.download(), o.get(), 3, "gyroid, strategy 3")
+
+
+def test_moment_field_strategy_limits():
+    """Strategy 3 writes the equilibrium, so it exists only for fully relaxing
+    lattices (tau = 1) without Lees-Edwards planes or inflow boundaries, and
+    needs two sites across x and y (a site and its periodic image in the
+    padded fields); elsewhere it is refused and the autotuner never offers
+    it."""
+    from lb3d_b200.lib import Lattice, Lb3dError
+    cases = [
+        (_params((16, 8, 8), 3, tau_r=0.8), 3),
+        (_params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=5, shear_u=0.05), 2),
+        (_params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=12, pr=0.01, pb=0.0, pg=0.0), 2),
+        (_params((1, 8, 8), 3), 3),
+    ]
+    for p, nc in cases:
+        lat = Lattice(p, precision=1)
+        lat.upload_state(uniform_mixture(p.nx, p.ny, p.nz, nc, seed=2))
+        with pytest.raises(Lb3dError):
+            lat.set_launch_shape(16, 8, 16, 3)
+        lat.autotune()
+        assert lat.launch_shape[3] != 3
