@@ -10,7 +10,7 @@
 //       moment fields:
 //         ternary  MF1 = {drho_r, drho_b, drho_s, P_x}
 //                  MF2 = {rho_b - rho_r, da}
-//                  plain MFp = {P_y, P_z}
+//                  plain MFp = {P_y, P_z}, plain DS = drho_s
 //         binary   MF1 = {drho_r, drho_b, P_x, P_y}, plain MFp = {P_z, 0}
 //       where P = sum_c amass_c omega_c j_c is the weighted momentum of
 //       code/lb3d_collision.F90:560-587 and da the advected dipole flux
@@ -103,12 +103,12 @@ struct MfGeom {
   static constexpr int FIELD = (BOX_BYTES + 127) / 128 * 128;
   // dipole pass: one MF2 box per slot, 5 slots
   static constexpr int D_SLOT = (FIELD + 1023) / 1024 * 1024;
-  static constexpr int D_RS = 5;
+  static constexpr int D_RS = 8;
   static constexpr int D_SMEM = D_RS * D_SLOT + 1024;
   // collide pass: MF1 (+ DD) boxes per slot, 6 slots; psi ring of 4 planes
   static constexpr int NF = NC == 3 ? 2 : 1;
   static constexpr int C_SLOT = (NF * FIELD + 1023) / 1024 * 1024;
-  static constexpr int C_RS = 6, PR = 4;
+  static constexpr int C_RS = 8, PR = 4;  // powers of two: cheap slot indices
   static constexpr int PSI_BYTES = PR * AN * (NC == 3 ? 16 : 8);
   static constexpr int C_SMEM = C_RS * C_SLOT + PSI_BYTES + 1024;
   static constexpr int AHEAD = 2;  // planes loaded ahead of use
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
     k_mf_moments(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                  const float *f0, const float *f1, const float *db0, const float *db1,
                  const uint8_t *__restrict__ rock, unsigned S, float4 *__restrict__ MF1,
-                 float4 *__restrict__ MF2, float2 *__restrict__ MFp) {
+                 float4 *__restrict__ MF2, float2 *__restrict__ MFp, float *__restrict__ DS) {
   constexpr int NT = TX * TY, DW = TX + 2, DN = DW * (TY + 2), DR = 4;
   extern __shared__ float4 smd[];  // previous dipoles [DR][DN] (ternary)
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
         }
         if (NC == 3) {
           MFp[self] = make_float2(p1, p2);
+          DS[self] = dr[NC - 1];
           mf_put(MF1, make_float4(dr[0], dr[1], dr[NC - 1], p0), gx, gy, gz, nx, ny);
           mf_put(MF2, make_float4(dr[1] - dr[0], a0, a1, a2), gx, gy, gz, nx, ny);
         } else {
@@ -270,10 +271,10 @@ __device__ __forceinline__ unsigned char *mf_smem_base(unsigned char *raw) {
 // LB3DC_ETIMEOUT if a plane never arrives.
 // ---------------------------------------------------------------------------
 template <int TX, int TY>
-__global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
+__global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
     k_mf_dipole(const __grid_constant__ CUtensorMap tm2, const LatDesc *__restrict__ lats,
                 const Tile *__restrict__ tiles, int ntiles, float *db0, float *db1,
-                const float4 *__restrict__ MF1, float4 *__restrict__ DD, int *err) {
+                const float *__restrict__ DS, float4 *__restrict__ DD, int *err) {
   using G = MfGeom<3, TX, TY>;
   constexpr int AW = G::AW, RS = G::D_RS, AHEAD = G::AHEAD;
   extern __shared__ unsigned char smraw_[];
@@ -309,6 +310,9 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
     if (tid == 0)
       for (int m = 0; m < AHEAD && m < npl; ++m) issue(m);
     issued = gbase + (unsigned)(AHEAD < npl ? AHEAD : npl);
+    // the own surfactant density deviation of the plane relaxed next,
+    // loaded one iteration ahead
+    float drs = 0.0f, drs_next = 0.0f;
     for (int j = 0; j < npl; ++j) {
       const unsigned g = gbase + (unsigned)j;
       const bool ok = mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
@@ -323,13 +327,10 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
         if (tid == 0) issue(j + AHEAD);
         issued = g + AHEAD + 1;
       }
+      if (act && j >= 1 && j <= zc) drs_next = __ldg(DS + gx + nx * (gy + ny * wrapz(z0 + j - 1, nz)));
       if (j >= 2 && act) {
         const int as = (tx + 1) + AW * (ty + 1);
         const int gz = wrapz(z0 + j - 2, nz);
-        const int XP = nx + 2 * MF_PAD, YP = ny + 2 * MF_PAD;
-        // the site's own surfactant density deviation
-        const float drs =
-            __ldg(MF1 + (size_t)XP * YP * gz + (gx + MF_PAD) + (size_t)XP * (gy + MF_PAD)).z;
         const float3 d = dipole_site<AW>(box(g - 2), box(g - 1), box(g), as, Lg, Lg.rho0, drs);
         const int i = gx + nx * (gy + ny * gz);
         __stcs(DBo + i, d.x);
@@ -337,6 +338,7 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
         __stcs(DBo + 2 * (size_t)Lg.nx * Lg.ny * Lg.nz + i, d.z);
         mf_put(DD, make_float4(d.x, d.y, d.z, 0.0f), gx, gy, gz, nx, ny);
       }
+      drs = drs_next;
     }
     if (failed) break;
     gbase += (unsigned)npl;
@@ -476,6 +478,9 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     if (tid == 0)
       for (int m = 0; m < AHEAD && m < npl; ++m) issue(m);
     issued = gbase + (unsigned)(AHEAD < npl ? AHEAD : npl);
+    // the own plain momentum entry of the plane collided next, loaded one
+    // iteration ahead
+    float2 op = make_float2(0.0f, 0.0f), op_next = op;
     for (int j = 0; j <= npl; ++j) {
       const unsigned g = gbase + (unsigned)j;
       bool ok = true;
@@ -506,6 +511,8 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
       }
       // ---- force and equilibrium of plane mc = j - 2 on the tile
       const int mc = j - 2;
+      if (act && mc + 1 >= 1 && mc + 1 <= zc)
+        op_next = __ldg(MFp + gx + nx * (gy + ny * wrapz(z0 + mc, nz)));
       if (mc >= 1 && mc <= zc && act) {
         const int gz = wrapz(z0 - 1 + mc, nz);
         Nbr nb;
@@ -531,7 +538,6 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
           }
           // own densities and weighted momentum
           const float4 o1 = box(gc, 0)[ap];
-          const float2 op = __ldg(MFp + self);
           float dr[NC], rho[NC], pp[3];
           if constexpr (NC == 3) {
             dr[0] = o1.x, dr[1] = o1.y, dr[NC - 1] = o1.z;
@@ -584,6 +590,7 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
                      Lg.omega[NC - 1]);
         }
       }
+      op = op_next;
     }
     if (failed) break;
     gbase += (unsigned)npl;

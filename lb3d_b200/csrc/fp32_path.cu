@@ -1049,7 +1049,7 @@ long long fp32_footprint(const lb3dc_params &p) {
   // the moment field of strategy 3 when every component relaxes fully
   const bool full = p.tau_r == 1.0 && p.tau_b == 1.0 && (p.ncomp == 2 || p.tau_s == 1.0);
   const long long mf = full && !le ? (long long)(p.nx + 2 * MF_PAD) * (p.ny + 2 * MF_PAD) * p.nz *
-                                             (p.ncomp == 3 ? 48 : 16) + N * 8
+                                             (p.ncomp == 3 ? 48 : 16) + N * 12
                                    : 0;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
          N * fp32_moment_bytes(p.ncomp) + mf +
@@ -1069,7 +1069,7 @@ bool fp32_mf_eligible(const DevParams &P) {
 
 long long fp32_mf_bytes(const DevParams &P) {
   return (long long)(P.nx + 2 * MF_PAD) * (P.ny + 2 * MF_PAD) * P.nz * (P.nc == 3 ? 48 : 16) +
-         P.nsites * 8 + 64;
+         P.nsites * (P.nc == 3 ? 12 : 8) + 64;
 }
 
 static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
@@ -1079,6 +1079,7 @@ static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
   if (ok && P.nc == 3) ok = cudaMalloc(&s.MF2, plane) == cudaSuccess;
   if (ok && P.nc == 3) ok = cudaMalloc(&s.DD, plane) == cudaSuccess;
   if (ok) ok = cudaMalloc(&s.MFp, (size_t)P.nsites * sizeof(float2)) == cudaSuccess;
+  if (ok && P.nc == 3) ok = cudaMalloc(&s.DS, (size_t)P.nsites * sizeof(float)) == cudaSuccess;
   if (ok && !s.err) ok = cudaMalloc(&s.err, sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
@@ -1086,8 +1087,10 @@ static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
     if (s.MF2) cudaFree(s.MF2);
     if (s.DD) cudaFree(s.DD);
     if (s.MFp) cudaFree(s.MFp);
+    if (s.DS) cudaFree(s.DS);
     s.MF1 = s.MF2 = s.DD = nullptr;
     s.MFp = nullptr;
+    s.DS = nullptr;
     return LB3DC_ENOMEM;
   }
   // padding entries that no site writes are read only by inactive lanes
@@ -1095,7 +1098,7 @@ static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
   if (s.MF2) cudaMemsetAsync(s.MF2, 0, plane, st);
   if (s.DD) cudaMemsetAsync(s.DD, 0, plane, st);
   cudaMemsetAsync(s.err, 0, sizeof(int), st);
-  s.bytes += (long long)plane * (P.nc == 3 ? 3 : 1) + P.nsites * 8;
+  s.bytes += (long long)plane * (P.nc == 3 ? 3 : 1) + P.nsites * (P.nc == 3 ? 12 : 8);
   return LB3DC_OK;
 }
 
@@ -1168,9 +1171,9 @@ static bool mf_fns(int nc, bool rock, bool body, int tx, int ty, bool narrow, co
 static size_t mf_smem(int nc, int tx, int ty, int which) {
   const size_t an = (size_t)(tx + 2) * (ty + 2), field = (16 * an + 127) / 128 * 128;
   if (which == 0) return nc == 3 ? 4 * an * 16 : 0;
-  if (which == 1) return 5 * ((field + 1023) / 1024 * 1024) + 1024;
+  if (which == 1) return 8 * ((field + 1023) / 1024 * 1024) + 1024;
   const size_t slot = ((nc == 3 ? 2 : 1) * field + 1023) / 1024 * 1024;
-  return 6 * slot + 4 * an * (nc == 3 ? 16 : 8) + 1024;
+  return 8 * slot + 4 * an * (nc == 3 ? 16 : 8) + 1024;
 }
 
 // One step of strategy 3: the moments pass, (ternary) the dipole pass and the
@@ -1198,12 +1201,12 @@ static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *ro
       const float *f0 = s.f[0], *f1 = s.f[1], *d0 = s.db[0], *d1 = s.db[1];
       void *args[] = {(void *)&dl, (void *)&dt, (void *)&ntl, (void *)&f0, (void *)&f1, (void *)&d0,
                       (void *)&d1, (void *)&rockp, (void *)&S, (void *)&s.MF1, (void *)&s.MF2,
-                      (void *)&s.MFp};
+                      (void *)&s.MFp, (void *)&s.DS};
       e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
     } else if (pass == 1) {
-      const float4 *mf1 = s.MF1;
+      const float *ds = s.DS;
       void *args[] = {(void *)&s.tm2, (void *)&dl, (void *)&dt, (void *)&ntl, (void *)&s.db[0],
-                      (void *)&s.db[1], (void *)&mf1, (void *)&s.DD, (void *)&s.err};
+                      (void *)&s.db[1], (void *)&ds, (void *)&s.DD, (void *)&s.err};
       e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
     } else {
       const float2 *mfp = s.MFp;
@@ -1510,10 +1513,12 @@ void fp32_free(Fp32State &s) {
   if (s.MF2) cudaFree(s.MF2);
   if (s.DD) cudaFree(s.DD);
   if (s.MFp) cudaFree(s.MFp);
+  if (s.DS) cudaFree(s.DS);
   if (s.err) cudaFree(s.err);
   if (s.mf_tiles) cudaFree(s.mf_tiles);
   s.MF1 = s.MF2 = s.DD = nullptr;
   s.MFp = nullptr;
+  s.DS = nullptr;
   s.mf_tiles = nullptr;
   s.err = nullptr;
   s.mf_tx = s.mf_ty = 0;

@@ -72,6 +72,7 @@ struct Fp32State {
   // of a wait that gave up
   float4 *MF1 = nullptr, *MF2 = nullptr, *DD = nullptr;
   float2 *MFp = nullptr;
+  float *DS = nullptr;
   int *err = nullptr;
   CUtensorMap tm1{}, tm2{}, tmd{};
   int mf_tx = 0, mf_ty = 0;
