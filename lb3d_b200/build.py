@@ -61,7 +61,7 @@ def build(verbose=False, force=False):
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(BUILD_DIR, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    objs, cmds = [], []
     for src, extra in SOURCES.items():
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
@@ -69,19 +69,21 @@ def build(verbose=False, force=False):
         obj = os.path.join(BUILD_DIR, src + ".o")
         objs.append(obj)
         if force or _stale(obj, path):
-            cmd = [nvcc] + ARCH + NVCC_COMMON + extra + ["-c", path, "-o", obj]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
+            cmds.append([nvcc] + ARCH + NVCC_COMMON + extra + ["-c", path, "-o", obj])
     for src, extra in CXX_SOURCES.items():
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD_DIR, src + ".o")
         objs.append(obj)
         if force or _stale(obj, path):
-            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"] + extra + ["-c", path, "-o", obj]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
+            cmds.append(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"] + extra + ["-c", path, "-o", obj])
+    # the translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    if verbose:
+        for cmd in cmds:
+            print(" ".join(cmd), flush=True)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.check_call, cmd) for cmd in cmds]:
+            f.result()
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         if verbose:

@@ -17,11 +17,20 @@
 //       (code/lb3d_advection.F90:137-148).
 //   k_mf_dipole (ternary): the dipole relaxation (code/lb3d_collision.F90:
 //       296-403) of every site from MF2 with a one-site halo, written to the
-//       dipole state and to the halo-padded dipole field DD = {d, 0}.
-//   k_mf_collide: psi deviations on the tile plus a one-site halo from MF1,
-//       the Shan-Chen force (code/lb3d_force_shanchen.F90:127-330) from them
-//       and (ternary) DD, the body force and the velocities, and the
+//       dipole state, and the site's force-stencil entry DD = {a, dpsi_s}
+//       with a = d psi(rho_s) (the product every neighbour's force term
+//       uses, code/lb3d_force_shanchen.F90:283) to a halo-padded field.
+//   k_mf_collide: psi deviations of red and blue on the tile plus a
+//       one-site halo from MF1, the Shan-Chen force
+//       (code/lb3d_force_shanchen.F90:127-330) from them and (ternary) DD and
+//       the own dipole, the body force and the velocities, and the
 //       populations of the next step.
+//
+// Lees-Edwards lattices (binary, no walls) run the same passes between the
+// FP32 path's halo kernels: the moments pass pulls across the sheared x
+// boundary from the stage-6 halo planes and the collide pass takes the psi
+// deviations of the x-halo columns from the stage-8 planes
+// (code/lb3d_bc_leesedwards.F90:147-1315).
 //
 // The padded fields carry two extra sites on each side in x and y; the
 // sites on an x or y boundary also write their periodic image into the
@@ -109,7 +118,7 @@ struct MfGeom {
   static constexpr int NF = NC == 3 ? 2 : 1;
   static constexpr int C_SLOT = (NF * FIELD + 1023) / 1024 * 1024;
   static constexpr int C_RS = 8, PR = 4;  // powers of two: cheap slot indices
-  static constexpr int PSI_BYTES = PR * AN * (NC == 3 ? 16 : 8);
+  static constexpr int PSI_BYTES = PR * AN * 8;
   static constexpr int C_SMEM = C_RS * C_SLOT + PSI_BYTES + 1024;
   static constexpr int AHEAD = 2;  // planes loaded ahead of use
   static constexpr int C_MINB = NT >= 256 ? 2 : 3;
@@ -140,7 +149,7 @@ __device__ __forceinline__ void mf_put(float4 *__restrict__ M, float4 e, int gx,
 // flux.  Binary lattices need no ring and their threads never wait on each
 // other.
 // ---------------------------------------------------------------------------
-template <int NC, int TX, int TY, bool ROCK, bool NARROW>
+template <int NC, int TX, int TY, bool ROCK, bool NARROW, bool LE = false>
 __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
     k_mf_moments(const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles,
                  const float *f0, const float *f1, const float *db0, const float *db1,
@@ -201,10 +210,19 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
         float a0 = 0.f, a1 = 0.f, a2 = 0.f;
         const float4 *Dm = smd + (it % DR) * DN, *D0 = smd + ((it + 1) % DR) * DN,
                      *Dp = smd + ((it + 2) % DR) * DN;
+        LeYZ lw;
+        if constexpr (LE) make_leyz(lw, gy, gz, ny, nz);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           float d[19];
-          pull_comp<ROCK, false, NARROW>(F, S, c, nb, self, rock, d);
+          // Lees-Edwards lattices pull across x = 0 and x = nx - 1 from the
+          // sheared halo planes of this step
+          if constexpr (LE) {
+            pull_comp_le<NARROW>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
+            le_store_boundary(Lg, 2, c, gx, gy, gz, d);  // for the stage-8 halo kernel
+          } else {
+            pull_comp<ROCK, false, NARROW>(F, S, c, nb, self, rock, d);
+          }
           own_moments<1>(d, dr[c], jm[c][0], jm[c][1], jm[c][2]);
           if (NC == 3 && c == 2) {
             // da = sum_q (n_s(x - c_q, q) g_q) db(x - c_q) + n_s(x, rest) db(x)
@@ -336,7 +354,10 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
         __stcs(DBo + i, d.x);
         __stcs(DBo + (size_t)Lg.nx * Lg.ny * Lg.nz + i, d.y);
         __stcs(DBo + 2 * (size_t)Lg.nx * Lg.ny * Lg.nz + i, d.z);
-        mf_put(DD, make_float4(d.x, d.y, d.z, 0.0f), gx, gy, gz, nx, ny);
+        const float pse = -Lg.em0 * expm1f(-drs);
+        const float ps = Lg.psi0 + pse;
+        const float2 a01 = mul2(make_float2(d.x, d.y), f2(ps));
+        mf_put(DD, make_float4(a01.x, a01.y, d.z * ps, pse), gx, gy, gz, nx, ny);
       }
       drs = drs_next;
     }
@@ -350,6 +371,82 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
       for (unsigned g = waited; g < issued; ++g) mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
     }
     __syncthreads();
+  }
+}
+
+// force_ternary with the neighbours' a = d (psi0 + dpsi_s) precomputed by the
+// dipole pass: psi entries {dpsi_r, dpsi_b}, a entries {a, dpsi_s}; the own
+// dipole d given.  The same operations in the same order as force_ternary.
+template <int W>
+__device__ __forceinline__ void force_ternary_pre(const float2 *Pm, const float2 *P0, const float2 *Pp,
+                                                  const float4 *Am, const float4 *A0, const float4 *Ap,
+                                                  int ap, float3 dd, const LatDesc &Lg, float psi0,
+                                                  float Fx[3][3]) {
+  float2 FB[3] = {f2(0.f), f2(0.f), f2(0.f)}, M01[3] = {f2(0.f), f2(0.f), f2(0.f)};
+  float2 TQ[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
+  float2 SA01 = f2(0.f);
+  float SA2 = 0.f, V[3] = {0, 0, 0}, M2[3] = {0, 0, 0}, SG = 0.f;
+#pragma unroll
+  for (int q = 0; q < 18; ++q) {
+    const float2 *Pq = cz(q) == 1 ? Pp : (cz(q) == -1 ? Pm : P0);
+    const float4 *Aq = cz(q) == 1 ? Ap : (cz(q) == -1 ? Am : A0);
+    const float g = (float)gw(q);
+    const int c[3] = {cx(q), cy(q), cz(q)};
+    const float2 e = Pq[ap + cx(q) + W * cy(q)];
+    const float4 av = Aq[ap + cx(q) + W * cy(q)];
+    const float2 a01 = make_float2(av.x, av.y);
+    const float a2 = av.z;
+    const float a[3] = {a01.x, a01.y, a2};
+    float ac = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (c[k]) ac = fmaf((float)c[k], a[k], ac);
+    const float Gq = g * (e.y - e.x);
+    const float g8 = 8.0f * g;
+    SG += Gq;
+    SA01 = fma2(f2(g), a01, SA01);
+    SA2 = fmaf(g, a2, SA2);
+    const float2 ezy = make_float2(e.y, e.x);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (c[k]) {
+        FB[k] = fma2(f2(g * (float)c[k]), ezy, FB[k]);
+        V[k] = fmaf(g * (float)c[k], ac, V[k]);
+        M01[k] = fma2(f2(g8 * (float)c[k]), a01, M01[k]);
+        M2[k] = fmaf(g8 * (float)c[k], a2, M2[k]);
+      }
+    }
+    const float2 gq = make_float2(Gq, g8 * ac);
+#define LB3D_SYM(I, J, K)                                  \
+  if (c[I] && c[J]) TQ[K] = fma2(gq, f2((float)(c[I] * c[J])), TQ[K]);
+    LB3D_SYM(0, 0, 0) LB3D_SYM(1, 1, 1) LB3D_SYM(2, 2, 2)
+    LB3D_SYM(0, 1, 3) LB3D_SYM(0, 2, 4) LB3D_SYM(1, 2, 5)
+#undef LB3D_SYM
+  }
+  const float frb[3] = {FB[0].x, FB[1].x, FB[2].x}, fbr[3] = {FB[0].y, FB[1].y, FB[2].y};
+  const float SA[3] = {SA01.x, SA01.y, SA2};
+  const float T[6] = {TQ[0].x, TQ[1].x, TQ[2].x, TQ[3].x, TQ[4].x, TQ[5].x};
+  const float Q[6] = {TQ[0].y, TQ[1].y, TQ[2].y, TQ[3].y, TQ[4].y, TQ[5].y};
+  const float M[3][3] = {{M01[0].x, M01[1].x, M01[2].x}, {M01[0].y, M01[1].y, M01[2].y},
+                         {M2[0], M2[1], M2[2]}};
+  const float d[3] = {dd.x, dd.y, dd.z};
+  const float2 own = P0[ap];
+  const float psr = psi0 + own.x, psb = psi0 + own.y, pss = psi0 + A0[ap].w;
+  auto dot3 = [&](float a0, float a1, float a2) { return fmaf(a2, d[2], fmaf(a1, d[1], a0 * d[0])); };
+  const float Td[3] = {dot3(T[0], T[3], T[4]), dot3(T[3], T[1], T[5]), dot3(T[4], T[5], T[2])};
+  const float Qd[3] = {dot3(Q[0], Q[3], Q[4]), dot3(Q[3], Q[1], Q[5]), dot3(Q[4], Q[5], Q[2])};
+  const float trM = M[0][0] + M[1][1] + M[2][2];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float MTd = dot3(M[0][k], M[1][k], M[2][k]);
+    const float Md = dot3(M[k][0], M[k][1], M[k][2]);
+    const float fcs = fmaf(-2.0f, V[k], SA[k]);
+    const float fsc = fmaf(SG, d[k], -2.0f * Td[k]);
+    const float fss = fmaf(-2.0f, Qd[k], fmaf(trM, d[k], MTd + Md));
+    const float cs = (-2.0f * Lg.g_bs) * fcs;
+    Fx[1][k] = fmaf(-Lg.g_br, fbr[k], cs) * psb;
+    Fx[0][k] = fmaf(-Lg.g_br, frb[k], -cs) * psr;
+    Fx[2][k] = fmaf(2.0f * Lg.g_bs, fsc, -Lg.g_ss * fss) * pss;
   }
 }
 
@@ -431,12 +528,12 @@ __device__ __forceinline__ void eq_store2(float *outA, float *outB, unsigned S, 
 // the ring's writers from its readers.  *err receives LB3DC_ETIMEOUT if a
 // plane never arrives.
 // ---------------------------------------------------------------------------
-template <int NC, int TX, int TY, bool ROCK, bool BODY>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false>
 __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     k_mf_collide(const __grid_constant__ CUtensorMap tm1, const __grid_constant__ CUtensorMap tmd,
                  const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles, float *f0,
-                 float *f1, const uint8_t *__restrict__ rock, unsigned S, const float2 *__restrict__ MFp,
-                 int *err) {
+                 float *f1, const float *db0, const float *db1, const uint8_t *__restrict__ rock, unsigned S,
+                 const float2 *__restrict__ MFp, int *err) {
   using G = MfGeom<NC, TX, TY>;
   constexpr int AW = G::AW, AN = G::AN, RS = G::C_RS, PR = G::PR, AHEAD = G::AHEAD;
   extern __shared__ unsigned char smraw_[];
@@ -465,6 +562,7 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     const LatDesc &Lg = sLat;
     const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz;
     float *__restrict__ Fo = Lg.parity ? f0 : f1;
+    const float *__restrict__ DBn = Lg.parity ? db0 : db1;
     const float psi0 = Lg.psi0, em0 = Lg.em0;
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
     const int npl = zc + 2;
@@ -481,6 +579,7 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     // the own plain momentum entry of the plane collided next, loaded one
     // iteration ahead
     float2 op = make_float2(0.0f, 0.0f), op_next = op;
+    float3 dnow = make_float3(0.f, 0.f, 0.f), dnext = dnow;
     for (int j = 0; j <= npl; ++j) {
       const unsigned g = gbase + (unsigned)j;
       bool ok = true;
@@ -500,19 +599,28 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
       if (j < npl) {
         const float4 *M1 = box(g, 0);
         for (int s = tid; s < AN; s += NT) {
+          if constexpr (LE) {
+            // the sheared halo columns take the psi deviations of the
+            // stage-8 halo planes (binary lattices)
+            const int vx = x0 - 1 + s % AW;
+            if (vx == -1 || vx == nx) {
+              const int iy = wrapz(y0 - 1 + s / AW, ny), iz = wrapz(z0 - 1 + j, nz);
+              reinterpret_cast<float2 *>(psiring)[(j % PR) * AN + s] = Lg.le_p[vx < 0 ? 0 : 1][iy + ny * iz];
+              continue;
+            }
+          }
           const float4 e = M1[s];
-          if constexpr (NC == 3)
-            reinterpret_cast<float4 *>(psiring)[(j % PR) * AN + s] =
-                make_float4(0.0f, -em0 * expm1f(-e.x), -em0 * expm1f(-e.y), -em0 * expm1f(-e.z));
-          else
-            reinterpret_cast<float2 *>(psiring)[(j % PR) * AN + s] =
-                make_float2(-em0 * expm1f(-e.x), -em0 * expm1f(-e.y));
+          reinterpret_cast<float2 *>(psiring)[(j % PR) * AN + s] =
+              make_float2(-em0 * expm1f(-e.x), -em0 * expm1f(-e.y));
         }
       }
       // ---- force and equilibrium of plane mc = j - 2 on the tile
       const int mc = j - 2;
-      if (act && mc + 1 >= 1 && mc + 1 <= zc)
-        op_next = __ldg(MFp + gx + nx * (gy + ny * wrapz(z0 + mc, nz)));
+      if (act && mc + 1 >= 1 && mc + 1 <= zc) {
+        const int in = gx + nx * (gy + ny * wrapz(z0 + mc, nz));
+        op_next = __ldg(MFp + in);
+        if (NC == 3) dnext = make_float3(__ldg(DBn + in), __ldg(DBn + S + in), __ldg(DBn + 2 * S + in));
+      }
       if (mc >= 1 && mc <= zc && act) {
         const int gz = wrapz(z0 - 1 + mc, nz);
         Nbr nb;
@@ -525,11 +633,10 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
           const unsigned gc = gbase + (unsigned)mc;
           float Fx[NC][3];
           if constexpr (NC == 3) {
-            const float4 *P4 = reinterpret_cast<const float4 *>(psiring);
-            force_ternary<AW, AW>(P4 + ((mc + PR - 1) % PR) * AN, P4 + (mc % PR) * AN,
-                                  P4 + ((mc + 1) % PR) * AN, DipF4{box(gc - 1, 1)}, DipF4{box(gc, 1)},
-                                  DipF4{box(gc + 1, 1)}, ap, ap, Lg, psi0,
-                                  reinterpret_cast<float(*)[3]>(Fx));
+            const float2 *P2 = reinterpret_cast<const float2 *>(psiring);
+            force_ternary_pre<AW>(P2 + ((mc + PR - 1) % PR) * AN, P2 + (mc % PR) * AN,
+                                  P2 + ((mc + 1) % PR) * AN, box(gc - 1, 1), box(gc, 1), box(gc + 1, 1), ap,
+                                  dnow, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
           } else {
             const float2 *P2 = reinterpret_cast<const float2 *>(psiring);
             force_binary<AW, ROCK>(P2 + ((mc + PR - 1) % PR) * AN, P2 + (mc % PR) * AN,
@@ -588,9 +695,24 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
           if (NC == 3)
             eq_store(fo + (size_t)38 * S, S, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1],
                      Lg.omega[NC - 1]);
+          if constexpr (LE) {
+            // the next step's pre-stream populations of the x boundary
+            // planes, for its stage-6 halo kernel (read back from the
+            // thread's own stores)
+            if (gx == 0 || gx == nx - 1) {
+#pragma unroll
+              for (int c = 0; c < NC; ++c) {
+                float v[19];
+#pragma unroll
+                for (int q = 0; q < 19; ++q) v[q] = fo[(size_t)(c * 19 + q) * S];
+                le_store_boundary(Lg, 0, c, gx, gy, gz, v);
+              }
+            }
+          }
         }
       }
       op = op_next;
+      dnow = dnext;
     }
     if (failed) break;
     gbase += (unsigned)npl;

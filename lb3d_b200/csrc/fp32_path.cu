@@ -291,6 +291,26 @@ __device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, unsign
 #undef LB3D_PULL_LE
 }
 
+// Writes one component's 19 deviations of a site on the x boundary of a
+// Lees-Edwards lattice to the compact boundary planes: set 0 (pre-stream,
+// le_b[0] at x = nx - 1, le_b[1] at x = 0) or set 2 (post-stream, le_b[2],
+// le_b[3]); sites elsewhere write nothing.
+__device__ __forceinline__ void le_store_boundary(const LatDesc &Lg, int set, int c, int gx, int gy,
+                                                  int gz, const float d[19]) {
+  const int nx = Lg.nx, NP = Lg.ny * Lg.nz;
+  const int o = (c * 19) * NP + gy + Lg.ny * gz;
+  if (gx == nx - 1) {
+    float *b = Lg.le_b[set] + o;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) b[q * NP] = d[q];
+  }
+  if (gx == 0) {
+    float *b = Lg.le_b[set + 1] + o;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) b[q * NP] = d[q];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // The fused kernel.  Grid: persistent CTAs over a tile list.  Populations
 // of lattice L live at f[(c*19+q)*S + L.base + site]; each component's
@@ -465,10 +485,15 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
 #pragma unroll
           for (int c = 0; c < NC; ++c) {
             float d[19];
-            if constexpr (LE)
+            if constexpr (LE) {
               pull_comp_le<NARROW>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
-            else
+              // the post-stream populations of the x boundary planes, for
+              // the stage-8 halo kernel
+              if (MODE == MODE_MOMENTS && x0 + ax < nx && y0 + ay < ny)
+                le_store_boundary(Lg, 2, c, gx, gy, gz, d);
+            } else {
               pull_comp<ROCK, false, NARROW>(F, S, c, nb, self, RK, d);
+            }
             if (MODE == MODE_MOMENTS) {
               own_moments<1>(d, dr[c], jm[c][0], jm[c][1], jm[c][2]);
             } else {
@@ -1048,19 +1073,19 @@ long long fp32_footprint(const lb3dc_params &p) {
   const long long np = (long long)p.ny * p.nz;
   // the moment field of strategy 3 when every component relaxes fully
   const bool full = p.tau_r == 1.0 && p.tau_b == 1.0 && (p.ncomp == 2 || p.tau_s == 1.0);
-  const long long mf = full && !le ? (long long)(p.nx + 2 * MF_PAD) * (p.ny + 2 * MF_PAD) * p.nz *
+  const long long mf = full ? (long long)(p.nx + 2 * MF_PAD) * (p.ny + 2 * MF_PAD) * p.nz *
                                              (p.ncomp == 3 ? 48 : 16) + N * 12
                                    : 0;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
          N * fp32_moment_bytes(p.ncomp) + mf +
-         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) : 0) + N * 8 + 4096;
+         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) + 4 * np * p.ncomp * 19 * 4 : 0) + N * 8 + 4096;
 }
 
 // ---------------------------------------------------------------------------
 // moment-field strategy (split 3): eligibility, field, tensor maps, launches
 // ---------------------------------------------------------------------------
 bool fp32_mf_eligible(const DevParams &P) {
-  if (P.le || P.invk) return false;
+  if ((P.le && P.nc != 2) || P.invk) return false;
   for (int c = 0; c < P.nc; ++c)
     if (P.omega[c] != 1.0) return false;
   if (P.nx < 2 || P.ny < 2) return false;
@@ -1138,30 +1163,36 @@ static int encode_mf_map(CUtensorMap *m, float4 *base, const DevParams &P, int t
   return r == CUDA_SUCCESS ? LB3DC_OK : LB3DC_ECUDA;
 }
 
-template <int NC, int TX, int TY, bool ROCK, bool BODY>
+template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE>
 static void mf_ptrs(bool narrow, const void **mom, const void **dip, const void **col) {
-  *mom = narrow ? (const void *)k_mf_moments<NC, TX, TY, ROCK, true>
-                : (const void *)k_mf_moments<NC, TX, TY, ROCK, false>;
+  *mom = narrow ? (const void *)k_mf_moments<NC, TX, TY, ROCK, true, LE>
+                : (const void *)k_mf_moments<NC, TX, TY, ROCK, false, LE>;
   *dip = NC == 3 ? (const void *)k_mf_dipole<TX, TY> : nullptr;
-  *col = (const void *)k_mf_collide<NC, TX, TY, ROCK, BODY>;
+  *col = (const void *)k_mf_collide<NC, TX, TY, ROCK, BODY, LE>;
 }
 // The kernels of strategy 3 for a lattice kind and tile shape (false if the
-// shape is not compiled); dip is null for binary lattices.
+// shape is not compiled); dip is null for binary lattices.  The
+// Lees-Edwards variants exist for binary lattices without walls.
 static bool mf_fns(int nc, bool rock, bool body, int tx, int ty, bool narrow, const void **mom,
-                   const void **dip, const void **col) {
-#define LB3D_MF(NC, R, B)                                                                \
-  if (tx == 32 && ty == 8) return mf_ptrs<NC, 32, 8, R, B>(narrow, mom, dip, col), true;   \
-  if (tx == 32 && ty == 4) return mf_ptrs<NC, 32, 4, R, B>(narrow, mom, dip, col), true;   \
-  if (tx == 16 && ty == 16) return mf_ptrs<NC, 16, 16, R, B>(narrow, mom, dip, col), true; \
-  if (tx == 16 && ty == 8) return mf_ptrs<NC, 16, 8, R, B>(narrow, mom, dip, col), true;   \
-  if (tx == 64 && ty == 4) return mf_ptrs<NC, 64, 4, R, B>(narrow, mom, dip, col), true;
+                   const void **dip, const void **col, bool le = false) {
+#define LB3D_MF(NC, R, B, L)                                                                   \
+  if (tx == 32 && ty == 8) return mf_ptrs<NC, 32, 8, R, B, L>(narrow, mom, dip, col), true;   \
+  if (tx == 32 && ty == 4) return mf_ptrs<NC, 32, 4, R, B, L>(narrow, mom, dip, col), true;   \
+  if (tx == 16 && ty == 16) return mf_ptrs<NC, 16, 16, R, B, L>(narrow, mom, dip, col), true; \
+  if (tx == 16 && ty == 8) return mf_ptrs<NC, 16, 8, R, B, L>(narrow, mom, dip, col), true;   \
+  if (tx == 64 && ty == 4) return mf_ptrs<NC, 64, 4, R, B, L>(narrow, mom, dip, col), true;
+  if (le) {
+    if (nc != 2 || rock) return false;
+    if (body) { LB3D_MF(2, false, true, true) } else { LB3D_MF(2, false, false, true) }
+    return false;
+  }
   if (nc == 3) {
     if (rock) return false;
-    if (body) { LB3D_MF(3, false, true) } else { LB3D_MF(3, false, false) }
+    if (body) { LB3D_MF(3, false, true, false) } else { LB3D_MF(3, false, false, false) }
   } else if (rock) {
-    if (body) { LB3D_MF(2, true, true) } else { LB3D_MF(2, true, false) }
+    if (body) { LB3D_MF(2, true, true, false) } else { LB3D_MF(2, true, false, false) }
   } else {
-    if (body) { LB3D_MF(2, false, true) } else { LB3D_MF(2, false, false) }
+    if (body) { LB3D_MF(2, false, true, false) } else { LB3D_MF(2, false, false, false) }
   }
 #undef LB3D_MF
   return false;
@@ -1173,24 +1204,37 @@ static size_t mf_smem(int nc, int tx, int ty, int which) {
   if (which == 0) return nc == 3 ? 4 * an * 16 : 0;
   if (which == 1) return 8 * ((field + 1023) / 1024 * 1024) + 1024;
   const size_t slot = ((nc == 3 ? 2 : 1) * field + 1023) / 1024 * 1024;
-  return 8 * slot + 4 * an * (nc == 3 ? 16 : 8) + 1024;
+  return 8 * slot + 4 * an * 8 + 1024;
 }
 
 // One step of strategy 3: the moments pass, (ternary) the dipole pass and the
-// collide pass, each on its own tile list and resident grid.
-static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *rockp, cudaStream_t st) {
+// collide pass, each on its own tile list and resident grid; with le (a
+// binary Lees-Edwards lattice) the stage-6 halo kernel runs before the
+// moments pass and the stage-8 one before the collide pass.
+static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *rockp, cudaStream_t st,
+                             const LEStep *le) {
   const bool rock = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
   const unsigned S = (unsigned)s.S;
   const bool narrow = 19ull * P.nc * s.S < (1ull << 32);
   const void *fn[3] = {nullptr, nullptr, nullptr};
-  if (!mf_fns(P.nc, rock, body, s.tx, s.ty, narrow, &fn[0], &fn[1], &fn[2]))
+  if (!mf_fns(P.nc, rock, body, s.tx, s.ty, narrow, &fn[0], &fn[1], &fn[2], le != nullptr))
     return cudaErrorInvalidConfiguration;
+  if (le && !s.le_h[0]) return cudaErrorInvalidValue;
+  const unsigned leg = (unsigned)((P.ny * P.nz + 63) / 64);
   if (s.mf_tx != s.tx || s.mf_ty != s.ty || !s.mf_tiles) return cudaErrorInvalidConfiguration;
   const int nt = s.tx * s.ty;
   const LatDesc *dl = s.d_lat;
   cudaError_t e = cudaSuccess;
   for (int pass = 0; pass < 3 && e == cudaSuccess; ++pass) {
     if (!fn[pass]) continue;
+    if (le && pass == 0) {
+      k_le_pre32<2><<<leg, 64, 0, st>>>(P, *le, dl, s.f[0], s.f[1], S);
+      if ((e = cudaGetLastError()) != cudaSuccess) break;
+    }
+    if (le && pass == 2) {
+      k_le_post32<2><<<leg, 64, 0, st>>>(P, *le, dl, s.f[0], s.f[1], S);
+      if ((e = cudaGetLastError()) != cudaSuccess) break;
+    }
     const size_t sm = mf_smem(P.nc, s.tx, s.ty, pass);
     int res = 0;
     if ((e = prepare_kernel(fn[pass], nt, sm, &res)) != cudaSuccess) break;
@@ -1211,8 +1255,8 @@ static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *ro
     } else {
       const float2 *mfp = s.MFp;
       void *args[] = {(void *)&s.tm1, (void *)&s.tmd, (void *)&dl, (void *)&dt, (void *)&ntl,
-                      (void *)&s.f[0], (void *)&s.f[1], (void *)&rockp, (void *)&S, (void *)&mfp,
-                      (void *)&s.err};
+                      (void *)&s.f[0], (void *)&s.f[1], (void *)&s.db[0], (void *)&s.db[1], (void *)&rockp,
+                      (void *)&S, (void *)&mfp, (void *)&s.err};
       e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
     }
   }
@@ -1242,7 +1286,7 @@ static int mf_chunks(int nz, int nxy, int resident, int halo) {
 static int mf_build_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaStream_t st) {
   const void *fn[3];
   if (!mf_fns(P.nc, (s.lat.flags & LAT_ROCK) != 0, (s.lat.flags & LAT_BODY) != 0, sh.tx, sh.ty,
-              19ull * P.nc * s.S < (1ull << 32), &fn[0], &fn[1], &fn[2]))
+              19ull * P.nc * s.S < (1ull << 32), &fn[0], &fn[1], &fn[2], s.le_h[0] != nullptr))
     return LB3DC_EINVAL;
   const LatDesc &L = s.lat;
   const int nxt = (L.nx + sh.tx - 1) / sh.tx, nyt = (L.ny + sh.ty - 1) / sh.ty, nxy = nxt * nyt;
@@ -1294,12 +1338,22 @@ int fp32_take_error(Fp32State &s, cudaStream_t st) {
   return v;
 }
 
+// Lees-Edwards lattices: the compact pre-stream boundary planes from the
+// current state (after an upload or a restore; the collide passes keep them
+// current from then on).
+static cudaError_t le_gather(const DevParams &P, Fp32State &s, cudaStream_t st) {
+  const long long n = (long long)P.nc * 19 * P.ny * P.nz;
+  k_le_gather32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s.d_lat, s.f[0], s.f[1], (unsigned)s.S);
+  return cudaGetLastError();
+}
+
 // The Lees-Edwards halo planes of a single lattice, referenced by its descriptor.
 static void attach_le(Fp32State &s) {
   for (int b = 0; b < 2; ++b) {
     s.lat.le_h[b] = s.le_h[b];
     s.lat.le_p[b] = s.le_p[b];
   }
+  for (int b = 0; b < 4; ++b) s.lat.le_b[b] = s.le_b[b];
 }
 
 // Shape before any autotuning: the split strategy with the staged collide
@@ -1334,7 +1388,7 @@ static int rebuild_tiles(const DevParams &P, Fp32State &s, const FusedShape &sh,
     if (!fp32_mf_eligible(P)) return LB3DC_ENOTSUP;
     const void *a, *b, *c;
     if (!mf_fns(P.nc, (s.lat.flags & LAT_ROCK) != 0, (s.lat.flags & LAT_BODY) != 0, sh.tx, sh.ty, true,
-                &a, &b, &c))
+                &a, &b, &c, s.le_h[0] != nullptr))
       return LB3DC_EINVAL;
     int rc = ensure_mf(P, s, st);
     if (rc) return rc;
@@ -1383,7 +1437,7 @@ int fp32_set_shape(const DevParams &P, Fp32State &s, const FusedShape &sh, cudaS
   if (!fused_fn(P.nc, false, false, sh)) return LB3DC_EINVAL;
   // Lees-Edwards lattices and lattices with inflow boundaries run the
   // staged split strategy only
-  if ((s.le_h[0] || s.lat.invk) && sh.split != 2) return LB3DC_ENOTSUP;
+  if ((s.le_h[0] && sh.split < 2) || (s.lat.invk && sh.split != 2)) return LB3DC_ENOTSUP;
   if (sh.split == 3 && !fp32_mf_eligible(P)) return LB3DC_ENOTSUP;
   if (sh.split && !s.M) return LB3DC_EINVAL;
   if (sh.split < 0 || sh.split > 3) return LB3DC_EINVAL;
@@ -1457,6 +1511,7 @@ int fp32_autotune(const DevParams &P, Fp32State &s, const uint8_t *rock, double 
   const int cur = s.lat.parity;
   cudaMemcpyAsync(s.f[cur], save, pop, cudaMemcpyDeviceToDevice, st);
   if (dbs) cudaMemcpyAsync(s.db[cur], (char *)save + pop, dbs, cudaMemcpyDeviceToDevice, st);
+  if (s.le_b[0]) le_gather(P, s, st);
   cudaStreamSynchronize(st);
   cudaFree(save);
   if (ntried) *ntried = n;
@@ -1492,6 +1547,11 @@ int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStre
           cudaMalloc(&s.le_p[b], np * sizeof(float2)) != cudaSuccess)
         return LB3DC_ENOMEM;
       s.bytes += (long long)(P.nc * 19 * np * sizeof(float) + np * sizeof(float2));
+    }
+    for (int b = 0; b < 4; ++b) {
+      if (cudaMalloc(&s.le_b[b], (size_t)P.nc * 19 * np * sizeof(float)) != cudaSuccess)
+        return LB3DC_ENOMEM;
+      s.bytes += (long long)(P.nc * 19 * np * sizeof(float));
     }
   }
   s.lat = fp32_make_desc(P, p.rho0 > 0 ? p.rho0 : 0.7, 0, false);
@@ -1530,6 +1590,10 @@ void fp32_free(Fp32State &s) {
     s.le_h[b] = nullptr;
     s.le_p[b] = nullptr;
   }
+  for (int b = 0; b < 4; ++b) {
+    if (s.le_b[b]) cudaFree(s.le_b[b]);
+    s.le_b[b] = nullptr;
+  }
   s.d_lat = nullptr;
   s.d_tiles = nullptr;
   s.M = nullptr;
@@ -1567,6 +1631,7 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   if (e != cudaSuccess) return LB3DC_ECUDA;
   if (cudaMemcpyAsync(s.d_lat, &s.lat, sizeof(LatDesc), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return LB3DC_ECUDA;
+  if (s.le_b[0] && le_gather(P, s, st) != cudaSuccess) return LB3DC_ECUDA;
   // keep the launch shape chosen so far (set or autotuned); the kernel
   // variant may change with the rock flag
   int rc = rebuild_tiles(P, s, FusedShape{s.tx, s.ty, s.zc, s.split}, st);
@@ -1660,11 +1725,10 @@ int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, 
   // kernels per step: the pass(es), two Lees-Edwards halo kernels, the parity flip
   const int passes = sh.split ? (P.nc == 3 ? 3 : 2) : 1;
   const int per_step = passes + (le ? 2 : 0) + 1;
-  if (sh.split == 3 && le) return LB3DC_ENOTSUP;
   for (int i = 0; i < nsteps; ++i) {
     if (s.timer) s.timer->start(st);
     cudaError_t e = sh.split == 3
-                        ? launch_mf(P, s, rock, st)
+                        ? launch_mf(P, s, rock, st, le)
                         : fp32_launch_fused(P.nc, rk, body, sh, s.d_lat, s.d_tiles, s.ntiles, 0,
                                             s.f[0], s.f[1], s.db[0], s.db[1], rock, s.S, st, s.M,
                                             s.J, le, &P);

@@ -38,6 +38,11 @@ struct LatDesc {
   float zh_in[2], zh_uz[3];
   float *le_h[2];
   float2 *le_p[2];
+  // Lees-Edwards boundary planes, [nc][19][nz][ny] deviations: le_b[0/1] the
+  // pre-stream populations at x = nx - 1 / x = 0 (written by the collide
+  // pass of the previous step), le_b[2/3] the post-stream populations there
+  // (written by the moments pass); the halo kernels read them coalesced
+  float *le_b[4];
 };
 constexpr int LAT_ROCK = 1, LAT_BODY = 2, LAT_ACTIVE = 4;
 
@@ -66,6 +71,7 @@ struct Fp32State {
   double *stage = nullptr;  // one FP64 population plane (N sites) for uploads and downloads
   float *le_h[2] = {nullptr, nullptr};  // Lees-Edwards halo planes (see LatDesc)
   float2 *le_p[2] = {nullptr, nullptr};
+  float *le_b[4] = {nullptr, nullptr, nullptr, nullptr};
   // moment-field strategy (split 3): the halo-padded moment fields (and
   // dipole field, ternary), the plain momentum plane, the tensor maps of their
   // TMA boxes (encoded for the tile shape mf_tx x mf_ty) and the device flag

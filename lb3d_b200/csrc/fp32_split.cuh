@@ -509,6 +509,17 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
             __stcs(fo + q * S, d01[q].x);
             __stcs(fo + (19 + q) * S, d01[q].y);
           }
+          if constexpr (LE) {
+            // the next step's pre-stream populations of the x boundary
+            // planes, for its stage-6 halo kernel
+            if (gx == 0 || gx == nx - 1) {
+              float v0[19], v1[19];
+#pragma unroll
+              for (int q = 0; q < 19; ++q) v0[q] = d01[q].x, v1[q] = d01[q].y;
+              le_store_boundary(Lg, 0, 0, gx, gy, gzc, v0);
+              le_store_boundary(Lg, 0, 1, gx, gy, gzc, v1);
+            }
+          }
         }
         if (NC == 3) {
           bgk_update(ds, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1], Lg.omega[NC - 1]);
@@ -556,25 +567,29 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
   const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base;
   const double rho0 = (double)Lg.rho0, f = L.lefrac;
   double hb[NC][19], ht[NC][19];
+  // the pre-stream populations of x = nx - 1 and x = 0 come from the compact
+  // boundary planes (consecutive threads read consecutive y)
+  (void)F;
+  (void)S;
   {
-    const int ia = (nx - 1) + nx * (y + ny * wrapz(z + L.eoff, nz));
-    const int ib = (nx - 1) + nx * (y + ny * wrapz(z + L.eoff + 1, nz));
+    const int ia = y + ny * wrapz(z + L.eoff, nz), ib = y + ny * wrapz(z + L.eoff + 1, nz);
+    const float *B = Lg.le_b[0];
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) {
         const double w = __dmul_rn(wq64(q), rho0);
-        hb[c][q] = (1.0 - f) * ((double)F[(size_t)(c * 19 + q) * S + ia] + w) +
-                   f * ((double)F[(size_t)(c * 19 + q) * S + ib] + w);
+        hb[c][q] = (1.0 - f) * ((double)B[(c * 19 + q) * NP + ia] + w) +
+                   f * ((double)B[(c * 19 + q) * NP + ib] + w);
       }
     le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
   }
   {
-    const int ia = nx * (y + ny * wrapz(z - L.eoff - 1, nz));
-    const int ib = nx * (y + ny * wrapz(z - L.eoff, nz));
+    const int ia = y + ny * wrapz(z - L.eoff - 1, nz), ib = y + ny * wrapz(z - L.eoff, nz);
+    const float *B = Lg.le_b[1];
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) {
         const double w = __dmul_rn(wq64(q), rho0);
-        ht[c][q] = f * ((double)F[(size_t)(c * 19 + q) * S + ia] + w) +
-                   (1.0 - f) * ((double)F[(size_t)(c * 19 + q) * S + ib] + w);
+        ht[c][q] = f * ((double)B[(c * 19 + q) * NP + ia] + w) +
+                   (1.0 - f) * ((double)B[(c * 19 + q) * NP + ib] + w);
       }
     le_adjust<NC>(P, ht, hb, L.shear_u, +1.0);
   }
@@ -596,20 +611,13 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
   const int y = t % ny, z = t / ny;
   const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base;
   const double rho0 = (double)Lg.rho0, f = L.lefrac;
-  // post-stream population q of component c at (x, yy, zz)
+  // post-stream population q of component c at (x, yy, zz), x = nx - 1 or
+  // 0: the moments pass left them in the compact boundary planes, pulled as
+  // it pulls every site (across x from the stage-6 halo planes)
+  (void)F;
+  (void)S;
   auto post = [&](int c, int q, int x, int yy, int zz) -> double {
-    float v;
-    if (q == 18) {
-      v = F[(size_t)(c * 19 + 18) * S + x + nx * (yy + ny * zz)];
-    } else {
-      const int xu = x - cx(q), yu = wrapz(yy - cy(q), ny), zu = wrapz(zz - cz(q), nz);
-      if (xu < 0)
-        v = Lg.le_h[0][(c * 19 + q) * NP + yu + ny * zu];
-      else if (xu >= nx)
-        v = Lg.le_h[1][(c * 19 + q) * NP + yu + ny * zu];
-      else
-        v = F[(size_t)(c * 19 + q) * S + xu + nx * (yu + ny * zu)];
-    }
+    const float v = Lg.le_b[x == 0 ? 3 : 2][(c * 19 + q) * NP + yy + ny * zz];
     return (double)v + __dmul_rn(wq64(q), rho0);
   };
   double hb[NC][19], ht[NC][19];
@@ -642,4 +650,20 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
   }
   Lg.le_p[0][t] = make_float2((float)dl[0], (float)dl[1]);
   Lg.le_p[1][t] = make_float2((float)dh[0], (float)dh[1]);
+}
+
+// Fills the compact pre-stream boundary planes from the state (after an
+// upload or a restored state); the collide passes keep them current after
+// every step.
+__global__ void k_le_gather32(const LatDesc *__restrict__ lat, const float *__restrict__ f0,
+                              const float *__restrict__ f1, unsigned S) {
+  const LatDesc &Lg = *lat;
+  const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)Lg.nc * 19 * NP) return;
+  const int cq = (int)(t / NP), yz = (int)(t % NP);
+  const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base + (size_t)cq * S;
+  const int row = nx * yz;  // y + ny * z
+  Lg.le_b[0][t] = F[row + nx - 1];
+  Lg.le_b[1][t] = F[row];
 }

@@ -15,6 +15,8 @@
 #include <mutex>
 #include <string>
 
+#include <cuda.h>
+
 #include "../../include/lb3dc.h"
 #include "common.cuh"
 #include "fp64_path.h"
@@ -30,6 +32,36 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[LB3DC_NOALLOC_S
 constexpr int kMaxDevices = 256;
 std::mutex g_mu;
 unsigned char *g_addr[kMaxDevices] = {nullptr};
+// The context each cached address belongs to: a device reset (or any
+// teardown of the primary context) reloads the module in a new context
+// with a new unique id, and the address is looked up again.
+unsigned long long g_ctx_id[kMaxDevices] = {0};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current context (0 if none or if the
+// driver offers no id), through the runtime's driver entry points.
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(a);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(b);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 inline size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -73,14 +105,17 @@ extern "C" int lb3dc_time_loop_fp64_noalloc(const lb3dc_params *p, double *f, do
   if (dev < 0 || dev >= kMaxDevices) return err(LB3DC_EINVAL, "device ordinal out of range");
   unsigned char *base;
   {
-    // Set-up, once per device and with that device current: the device
+    // Set-up, once per device (and again after the device's context was
+    // torn down and recreated) with that device current: the device
     // address of the scratch array.
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    const unsigned long long id = current_ctx_id();
+    if (!g_addr[dev] || id == 0 || id != g_ctx_id[dev]) {
       void *ptr = nullptr;
       e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (e != cudaSuccess) return err(LB3DC_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       g_addr[dev] = (unsigned char *)ptr;
+      g_ctx_id[dev] = current_ctx_id();  // the lookup made the context current
     }
     base = g_addr[dev];
   }

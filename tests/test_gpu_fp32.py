@@ -302,14 +302,13 @@ def test_moment_field_strategy_against_oracle():
 
 def test_moment_field_strategy_limits():
     """Strategy 3 writes the equilibrium, so it exists only for fully relaxing
-    lattices (tau = 1) without Lees-Edwards planes or inflow boundaries, and
-    needs two sites across x and y (a site and its periodic image in the
-    padded fields); elsewhere it is refused and the autotuner never offers
-    it."""
+    lattices (tau = 1) without inflow boundaries, and needs two sites across
+    x and y (a site and its periodic image in the padded fields); elsewhere
+    it is refused and the autotuner never offers it."""
     from lb3d_b200.lib import Lattice, Lb3dError
     cases = [
         (_params((16, 8, 8), 3, tau_r=0.8), 3),
-        (_params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=5, shear_u=0.05), 2),
+        (_params((16, 8, 8), 2, tau_b=1.2, boundary_cond=-1, inv_fluid=5, shear_u=0.05), 2),
         (_params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=12, pr=0.01, pb=0.0, pg=0.0), 2),
         (_params((1, 8, 8), 3), 3),
     ]
@@ -320,3 +319,32 @@ def test_moment_field_strategy_limits():
             lat.set_launch_shape(16, 8, 16, 3)
         lat.autotune()
         assert lat.launch_shape[3] != 3
+
+
+@pytest.mark.parametrize("shear_u,omega", [(0.05, 0.0), (-0.3, 0.0), (0.2, 0.31)])
+@pytest.mark.parametrize("dims,shape", [((40, 12, 20), (32, 4, 16)), ((8, 6, 10), (16, 8, 16)),
+                                        ((64, 24, 18), (64, 4, 16))])
+def test_moment_field_strategy_lees_edwards_equals_staged_split(dims, shape, shear_u, omega):
+    """Binary Lees-Edwards lattices on strategy 3 (pulls across the sheared
+    x boundary in the moments pass, the stage-8 halo psi columns in the
+    collide pass) give strategy 2's bits for positive, negative and
+    oscillating plane offsets, and the oracle's within the tolerances."""
+    from lb3d_b200.lib import Lattice
+    p = _params(dims, 2, boundary_cond=-1, inv_fluid=5, shear_u=shear_u, shear_omega=omega,
+                g_accn_x=1e-5)
+    st = uniform_mixture(*dims, 2, seed=5)
+    st["shear_sum"] = 0.37
+    out = []
+    for split in (2, 3):
+        lat = Lattice(p, precision=1)
+        lat.upload_state(st)
+        lat.set_launch_shape(*shape, split)
+        lat.time_loop(15)
+        lat.sync()
+        out.append(lat.download())
+        shear_sum = lat.lees_edwards[0]
+    assert np.array_equal(out[0]["n"], out[1]["n"])
+    o = Oracle(p, st)
+    o.run(15)
+    check(out[1], o.get(), 2, f"LE strategy 3 {dims} shear_u={shear_u}")
+    assert shear_sum == o.shear_sum
