@@ -36,12 +36,24 @@ METRIC = "ternary D3Q19 MLUPS & %HBM peak, FP32-dev vs FP64; ensemble solves/s, 
 L = 128
 BYTES_PER_SITE = {("f32", 3): 480, ("f32", 2): 304, ("f64", 3): 960, ("f64", 2): 608}
 # DRAM bytes per site and step that ncu measured (dram__bytes_read.sum +
-# dram__bytes_write.sum of the moments, dipole and staged collide passes) on
-# the ternary 128^3 workload, keyed by (tile x, tile y, strategy); captured
-# with 8-plane chunks (the chunk depth moves only the ring halo reloads,
-# under 1 % of this figure).
-NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 772}
+# dram__bytes_write.sum summed over the step's passes) on the ternary 128^3
+# workload: strategy 2 (moments, dipole and staged collide passes; 32x4
+# tiles, 8-plane chunks) and strategy 3 (moments, dipole and TMA-fed collide
+# passes; 32x8 tiles).  Keyed by (tile x, tile y, strategy); for strategy 3
+# the tile shape moves only halo reloads that hit L2, so its figure stands
+# for every shape.
+NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 772, (32, 8, 3): 549}
+
+
+def ncu_traffic(shape):
+    key = (shape[0], shape[1], shape[3])
+    if key in NCU_TRAFFIC_PER_SITE:
+        return NCU_TRAFFIC_PER_SITE[key]
+    if shape[3] == 3:
+        return NCU_TRAFFIC_PER_SITE[(32, 8, 3)]
+    return None
 PHYS = dict(tau_d=1.0, g_br=0.08, g_bs=-0.006, g_ss=-0.0045, beta=10.0, d_0=1.0, bdist=2, restore=1)
+STRATEGIES = ["fused", "split", "split, staged collide", "moment field, TMA-fed collide"]
 
 
 def measured_peak():
@@ -133,9 +145,23 @@ def cpu_baseline(threads, seconds_target=15.0):
             "sample": f"ternary {L}^3 FP64 CPU restatement, {steps} full steps ({dt:.1f} s), OpenMP"}
 
 
+def workload_config(world=1):
+    """The `config` of the headline line, shared by both arms."""
+    return {"workload": f"ternary D3Q19 {L}^3 periodic", "lattice": [L, L, L], "g_br": 0.08, "g_bs": -0.006,
+            "g_ss": -0.0045, "tau": 1.0, "tau_d": 1.0, "beta": 10.0, "parallelism": f"replicas x{world}",
+            "l2": f"populations {2 * 57 * 4 * L ** 3 / 1e6:.0f} MB > 126 MB L2, no flush"}
+
+
+# The CPU arm runs every requested step unless that would take longer than
+# this (a 128^3 ternary FP64 step takes ~0.35 s on 16 cores).
+REFERENCE_BUDGET_S = 300.0
+
+
 def run_reference(args):
     """--impl reference: the CPU restatement of the reference's path on all
-    host threads, same workload and metric; rank 0 only."""
+    host threads, same workload, metric, steps and warm-up; rank 0 only.  The
+    reference's own Fortran/MPI build cannot be compiled on either machine
+    (no gfortran, MPI or rpc/xdr.h)."""
     from lb3d_b200.dist import world
     rank, _, size = world()
     if rank != 0:
@@ -145,51 +171,74 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     p = workload_params(precision=0)
     o = Oracle(p, uniform_mixture(L, L, L, 3, seed=1), threads=threads)
-    o.run(max(1, min(args.warmup, 3)))
-    steps = max(1, min(args.steps, 10))
+    t0 = time.perf_counter()
+    o.run(1)
+    est = time.perf_counter() - t0
+    warm = max(0, min(args.warmup, int(REFERENCE_BUDGET_S / 4 / est)) - 1)
+    o.run(warm)
+    steps = max(1, min(args.steps, int(REFERENCE_BUDGET_S / est)))
     t0 = time.perf_counter()
     o.run(steps)
     dt = time.perf_counter() - t0
     v = L ** 3 * steps / dt / 1e6
+    sample = (f"full {L}^3 lattice, {steps} steps after {warm + 1} warm-up steps, C++ restatement of the "
+              "reference's FP64 path (OpenMP); the reference's Fortran/MPI build is unavailable on this "
+              "machine (no gfortran, MPI or rpc/xdr.h)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MLUPS",
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / steps, 3),
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm + 1, "ms_per_step": round(1e3 * dt / steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"ternary D3Q19 {L}^3 periodic (FP64, CPU)", "lattice": [L, L, L]},
+        "config": workload_config(size),
+        "steps_capped": steps < args.steps,
         "cpu_baseline": {"value": round(v, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
-                         "sample": f"full {L}^3 lattice, {steps} steps; the reference's Fortran/MPI build is "
-                                   "unavailable in this image (no gfortran, no MPI), so its C++ restatement runs"},
+                         "sample": sample},
         "e2e": {"value": round(v, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
-def time_lattice(lat, steps, warmup, sampler=None):
+def time_lattice(lat, steps, warmup, sampler=None, min_s=0.0, max_blocks=400):
+    """Times blocks of exactly `steps` steps with CUDA events on the
+    lattice's stream after `warmup` untimed steps.  With min_s > 0 blocks
+    repeat until that much device time has passed, so that a clock sampler
+    running meanwhile records the clocks under this load.  Returns the
+    median block's device ms, the kernel ms and launches per block
+    (bracketed dominant kernels), all launches per block, and the block count."""
     import torch
     st = torch.cuda.ExternalStream(lat.stream)
     lat.time_loop(warmup)
     lat.sync()
-    lat.set_profiling(True)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    blocks, kms_tot, kl_tot, all_tot = [], 0.0, 0, 0
     if sampler:
         sampler.recording = True
-    e0.record(st)
-    lat.time_loop(steps)
-    e1.record(st)
-    e1.synchronize()
+    while True:
+        lat.set_profiling(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lat.time_loop(steps)
+        e1.record(st)
+        e1.synchronize()
+        blocks.append(e0.elapsed_time(e1))
+        kms, klaunch, alllaunch = lat.kernel_stats()
+        lat.set_profiling(False)
+        kms_tot, kl_tot, all_tot = kms_tot + kms, kl_tot + klaunch, all_tot + alllaunch
+        if sum(blocks) >= 1e3 * min_s or len(blocks) >= max_blocks:
+            break
     if sampler:
         sampler.recording = False
-    wall_ms = e0.elapsed_time(e1)
-    kms, klaunch, alllaunch = lat.kernel_stats()
-    lat.set_profiling(False)
-    return wall_ms, kms, klaunch, alllaunch
+    n = len(blocks)
+    return statistics.median(blocks), kms_tot / n, kl_tot / n, all_tot // n, n
 
 
-def serving(rank, size, nreq=96, seq_sample=4):
+def serving(rank, size, nreq=96, seq_sample=6):
     """The serving ensemble on this rank's share of a seeded Poisson stream
     of ternary parameter-sweep solves (mean 200 req/s, cubic edges
     log-uniform 16..96, steps 500..5000), continuous batching by HBM
-    footprint; and sequential solves of the first requests through the FP64
-    plain path and the single-lattice FP32 path for comparison."""
+    footprint; and sequential solves of `seq_sample` requests spread evenly
+    over the stream through the FP64 plain path and the single-lattice FP32
+    path.  Both sides are compared in site updates per second (the requests
+    differ in size and step count), and the sampled requests also give the
+    FP32-vs-FP64 density gap at their last step beside the FP64 path's own
+    sensitivity (FP64 from populations perturbed by 1e-7 relative)."""
     from lb3d_b200.dist import partition
     from lb3d_b200.ensemble import Ensemble, Server, sweep_requests
     from lb3d_b200.ic import uniform_mixture
@@ -199,7 +248,10 @@ def serving(rank, size, nreq=96, seq_sample=4):
     out = Server(ens, chunk=512, download=True, on_result=lambda r, res: None).run(reqs)
     ens.close()
     seq = {}
-    sample = reqs[:seq_sample]
+    k = max(1, len(reqs) // max(1, seq_sample))
+    sample = reqs[::k][:seq_sample]
+    su = sum(r.params.nx * r.params.ny * r.params.nz * r.steps for r in sample)
+    finals = {}
     for prec, name in ((0, "fp64_plain"), (1, "fp32_single")):
         t = 0.0
         for r in sample:
@@ -209,11 +261,27 @@ def serving(rank, size, nreq=96, seq_sample=4):
             t0 = time.perf_counter()
             lat.upload_state(st)
             lat.time_loop(r.steps)
-            lat.download()
+            res = lat.download()
             t += time.perf_counter() - t0
             lat.close()
-        seq[name] = len(sample) / t
-    return out, seq, len(sample)
+            finals[(name, r.rid)] = res["rho"]
+        seq[name] = {"solves_per_s": len(sample) / t, "site_updates_per_s": su / t}
+    # accuracy of the FP32 solves against FP64, beside FP64's own sensitivity
+    gap, floor = 0.0, 0.0
+    for r in sample:
+        p = r.params
+        st = uniform_mixture(p.nx, p.ny, p.nz, 3, seed=r.seed)
+        st["n"] = st["n"] * (1.0 + 1e-7 * (2.0 * np.random.default_rng(r.seed).random(st["n"].shape) - 1.0))
+        lat = Lattice(p, precision=0)
+        lat.upload_state(st)
+        lat.time_loop(r.steps)
+        pert = lat.download()["rho"]
+        lat.close()
+        ref = finals[("fp64_plain", r.rid)]
+        gap = max(gap, float(np.abs(finals[("fp32_single", r.rid)] - ref).max()))
+        floor = max(floor, float(np.abs(pert - ref).max()))
+    seq["accuracy"] = {"max_abs_drho_fp32_vs_fp64": gap, "max_abs_drho_fp64_perturbed_1e-7": floor}
+    return out, seq, [r.rid for r in sample]
 
 
 def run_configs(args):
@@ -233,7 +301,7 @@ def run_configs(args):
         shape = None
         if prec == 1 and tune:
             shape, _ = lat.autotune()
-        w, k, n, _ = time_lattice(lat, steps, 5)
+        w, k, n, _, _ = time_lattice(lat, steps, 5)
         lat.close()
         return p.nx * p.ny * p.nz * steps / (w * 1e-3) / 1e6, shape
 
@@ -247,29 +315,15 @@ def run_configs(args):
     v, _ = mlups(p1, st1, 0, 1000)
     line({"case": "binary-64", "workload": "binary 64^3 periodic FP64 plain, 1000 steps", "mlups": round(v, 1),
           "frac": round(v * 1e6 * 608 / 1e9 / peak, 4), "bytes_per_site": 608})
-    # ternary 128^3, FP64 vs FP32 deviation error after 1k and 10k steps
+    # ternary 128^3: FP32 (autotuned strategy) and FP64
     p2 = workload_params(precision=0)
     st2 = uniform_mixture(L, L, L, 3, seed=1)
-    a = Lattice(p2, precision=0)
-    b = Lattice(p2, precision=1)
-    a.upload_state(st2)
-    b.upload_state(st2)
-    b.autotune()
-    done = 0
-    for target in (1000, args.error_steps):
-        a.time_loop(target - done)
-        b.time_loop(target - done)
-        done = target
-        ra, rb = a.download(), b.download()
-        d = np.abs(ra["rho"] - rb["rho"])
-        phi_a, phi_b = ra["rho"][0] - ra["rho"][1], rb["rho"][0] - rb["rho"][1]
-        line({"case": "ternary-128-error", "steps": target, "workload": "ternary 128^3, FP32-deviation vs FP64 plain",
-              "max_abs_drho": float(d.max()), "rms_drho": float(np.sqrt((d ** 2).mean())),
-              "max_abs_dphi": float(np.abs(phi_a - phi_b).max()),
-              "rho_range_fp64": [float(ra["rho"].min()), float(ra["rho"].max())],
-              "max_abs_ddb": float(np.abs(ra["db"] - rb["db"]).max())})
-    a.close()
-    b.close()
+    v32, shape2 = mlups(p2, st2, 1, 200, tune=True)
+    v64, _ = mlups(p2, st2, 0, 200)
+    line({"case": "ternary-128", "workload": "ternary 128^3 periodic, FP32 deviation and FP64 plain",
+          "mlups_fp32": round(v32, 1), "frac_fp32": round(v32 * 1e6 * 480 / 1e9 / peak, 4),
+          "mlups_fp64": round(v64, 1), "frac_fp64": round(v64 * 1e6 * 960 / 1e9 / peak, 4),
+          "launch_shape": shape2})
     # binary Lees-Edwards 256x128x128 (x-planes sheared), shear 0.05
     p3 = Params(nx=256, ny=128, nz=128, ncomp=2, boundary_cond=-1, inv_fluid=5, shear_u=0.05,
                 **phys2).finalize()
@@ -295,6 +349,117 @@ def run_configs(args):
           "frac_fp32": round(v32 * 1e6 * (304 * nf + 1) / 1e9 / peak, 4), "launch_shape": shape})
 
 
+def _velocity(res, fluid):
+    """Barycentric velocity sum_c j_c / sum_c rho_c at fluid sites (0 elsewhere)."""
+    rho = res["rho"].sum(0)
+    mom = res["mom"].sum(0)
+    u = np.where(fluid[None] & (rho[None] > 0), mom / np.where(rho > 0, rho, 1.0)[None], 0.0)
+    return u
+
+
+def _structure_k1(phi):
+    """First moment k1 = sum |k| S(k) / sum S(k) of the structure factor of
+    the order parameter (k = 0 excluded); 2 pi / k1 is the mean domain size."""
+    f = np.fft.fftn(phi - phi.mean())
+    s = (f * np.conj(f)).real
+    ks = [2 * np.pi * np.fft.fftfreq(n) for n in phi.shape]
+    kz, ky, kx = np.meshgrid(*ks, indexing="ij")
+    k = np.sqrt(kx * kx + ky * ky + kz * kz)
+    m = k > 0
+    return float((k[m] * s[m]).sum() / s[m].sum())
+
+
+def _hist(phi):
+    h, _ = np.histogram(phi, bins=64, range=(-1.5, 1.5))
+    return h / max(1, h.sum())
+
+
+def run_accuracy(args):
+    """--accuracy: the FP32 deviation path against the FP64 plain path on the
+    benchmark workloads, beside the FP64 path's own sensitivity (FP64 started
+    from populations perturbed by 1e-7 relative), at several step counts:
+    max and rms |drho|, |dphi| (phi = rho_r - rho_b) and |du| (barycentric
+    velocity), plus one statistical observable per workload (the first
+    moment of the order parameter's structure factor and the L1 distance of
+    its histogram for the phase-separating mixtures, the Darcy flux for the
+    porous one).  A mixed (non-phase-separating) ternary lattice is added,
+    where the pointwise bound can hold for any number of steps.  The FP64
+    path is bit-identical to the oracle, so it stands in for it here."""
+    import torch
+    from lb3d_b200.config import Params
+    from lb3d_b200.ic import invasion_state, sphere_pack, uniform_mixture
+    from lb3d_b200.lib import Lattice
+    torch.cuda.set_device(0)
+    phys2 = dict(tau_d=1.0, beta=10.0, d_0=1.0, bdist=2, restore=1, g_br=0.08)
+    cases = []
+    if "ternary-128" in args.accuracy_cases:
+        cases.append(("ternary-128", workload_params(precision=0), lambda: uniform_mixture(L, L, L, 3, seed=1),
+                      [1000, 10000]))
+    if "mixed-64" in args.accuracy_cases:
+        pm = Params(nx=64, ny=64, nz=64, ncomp=3, **{**PHYS, "g_br": args.mixed_g_br}).finalize()
+        cases.append(("ternary-64-mixed", pm, lambda: uniform_mixture(64, 64, 64, 3, seed=2), [1000, 10000]))
+    if "lees-edwards" in args.accuracy_cases:
+        p3 = Params(nx=256, ny=128, nz=128, ncomp=2, boundary_cond=-1, inv_fluid=5, shear_u=0.05,
+                    **phys2).finalize()
+        cases.append(("lees-edwards-256x128x128", p3, lambda: uniform_mixture(256, 128, 128, 2, seed=3),
+                      [1000, 10000, 20000]))
+    if "porous" in args.accuracy_cases:
+        p4 = Params(nx=256, ny=256, nz=256, ncomp=2, g_accn_x=1e-5, **phys2).finalize()
+        rock = sphere_pack(256, 256, 256, seed=4, porosity=0.4, rmin=6, rmax=12, overlap=True)
+        cases.append(("porous-256", p4, lambda: invasion_state(256, 256, 256, rock, seed=4), [1000, 10000, 20000]))
+    for name, p, make, marks in cases:
+        st = make()
+        fluid = st["rock"] == 0
+        pert = dict(st)
+        rng = np.random.default_rng(99)
+        pert["n"] = st["n"] * (1.0 + 1e-7 * (2.0 * rng.random(st["n"].shape) - 1.0))
+        a, b, c = Lattice(p, precision=0), Lattice(p, precision=0), Lattice(p, precision=1)
+        a.upload_state(st)
+        b.upload_state(pert)
+        c.upload_state(st)
+        shape, _ = c.autotune()
+        del pert
+        done = 0
+        for target in marks:
+            for lat in (a, b, c):
+                lat.time_loop(target - done)
+            done = target
+            ra = a.download()
+            out = {"case": name, "steps": target, "fp32_launch_shape": list(shape)}
+            ua = _velocity(ra, fluid)
+            phia = ra["rho"][0] - ra["rho"][1]
+            for tag, lat in (("fp32", c), ("fp64_perturbed", b)):
+                r = lat.download()
+                d = np.abs(r["rho"] - ra["rho"])
+                dphi = np.abs((r["rho"][0] - r["rho"][1]) - phia)
+                du = np.abs(_velocity(r, fluid) - ua)
+                m = {"max_abs_drho": float(d.max()), "rms_drho": float(np.sqrt((d ** 2).mean())),
+                     "max_abs_dphi": float(dphi.max()), "rms_dphi": float(np.sqrt((dphi ** 2).mean())),
+                     "max_abs_du": float(du.max()), "rms_du": float(np.sqrt((du ** 2).mean()))}
+                phi = r["rho"][0] - r["rho"][1]
+                if name.startswith("porous"):
+                    qa = float(ua[0].sum() / ua[0].size)
+                    q = float(_velocity(r, fluid)[0].sum() / ua[0].size)
+                    m["darcy_flux"] = q
+                    m["darcy_flux_rel_diff"] = abs(q - qa) / max(abs(qa), 1e-30)
+                else:
+                    k1a, k1 = _structure_k1(phia), _structure_k1(phi)
+                    m["structure_k1"] = k1
+                    m["structure_k1_rel_diff"] = abs(k1 - k1a) / k1a
+                    m["phi_hist_l1"] = float(np.abs(_hist(phi) - _hist(phia)).sum())
+                out[tag] = m
+                del r
+            if name.startswith("porous"):
+                out["fp64"] = {"darcy_flux": float(ua[0].sum() / ua[0].size)}
+            else:
+                out["fp64"] = {"structure_k1": _structure_k1(phia),
+                               "phi_range": [float(phia.min()), float(phia.max())]}
+            print(json.dumps(out), flush=True)
+            del ra
+        for lat in (a, b, c):
+            lat.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -306,7 +471,10 @@ def main():
     ap.add_argument("--requests", type=int, default=96)
     ap.add_argument("--configs", action="store_true", help="measure the four single-lattice workloads (binary 64^3 FP64, ternary 128^3 FP32 error, "
                     "Lees-Edwards 256x128x128, porous 256^3) instead")
-    ap.add_argument("--error-steps", type=int, default=10000)
+    ap.add_argument("--accuracy", action="store_true", help="FP32 vs FP64 error and the FP64 sensitivity "
+                    "floor on the benchmark workloads, with statistical observables")
+    ap.add_argument("--accuracy-cases", default="ternary-128,mixed-64,lees-edwards,porous")
+    ap.add_argument("--mixed-g-br", type=float, default=0.02)
     ap.add_argument("--shape", default=None,
                     help="tx,ty,zc,split: fixed FP32 launch shape instead of the autotuner (profiling runs)")
     args = ap.parse_args()
@@ -315,6 +483,8 @@ def main():
         return run_reference(args)
     if args.configs:
         return run_configs(args)
+    if args.accuracy:
+        return run_accuracy(args)
 
     import torch
     from lb3d_b200 import dist as D
@@ -340,8 +510,11 @@ def main():
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
+    # blocks of exactly `steps` steps repeat for >= 2 s so that the clock
+    # sampler (50 ms period) sees the load; the line reports the median block
     with ClockSampler(local) as clk:
-        wall_ms, kms, klaunch, alllaunch = time_lattice(lat, args.steps, args.warmup, clk)
+        wall_ms, kms, klaunch, alllaunch, nblocks = time_lattice(lat, args.steps, args.warmup, clk,
+                                                                 min_s=2.0)
     wall_ms, kms = D.max_over_ranks([wall_ms, kms], dev)
     ms_step = wall_ms / args.steps
     value = world * N * args.steps / (wall_ms * 1e-3) / 1e6
@@ -354,7 +527,7 @@ def main():
     lat64 = Lattice(workload_params(precision=0))
     lat64.upload_state(state)
     s64 = max(20, args.steps // 5)
-    w64, k64, n64, _ = time_lattice(lat64, s64, 3)
+    w64, k64, n64, _, _ = time_lattice(lat64, s64, 3)
     (w64,) = D.max_over_ranks([w64], dev)
     v64 = world * N * s64 / (w64 * 1e-3) / 1e6
     lat64.close()
@@ -388,18 +561,28 @@ def main():
     # ---- serving ensemble ----
     serve = None
     if not args.no_serving:
-        out, seq, nseq = serving(rank, world, args.requests)
+        out, seq, sample_ids = serving(rank, world, args.requests)
         wall, = D.max_over_ranks([out["wall_s"]], dev)
         solves, su = D.sum_over_ranks([out["solves"], out["site_updates"]], dev)
         p99, = D.max_over_ranks([out["p99_s"]], dev)
+        s64u = world * seq["fp64_plain"]["site_updates_per_s"]
         serve = {"requests": args.requests, "solves_per_s": round(solves / wall, 3),
                  "p50_s": round(out["p50_s"], 3), "p99_s": round(p99, 3),
                  "glups": round(su / wall / 1e9, 3),
-                 "sequential_fp64_plain_solves_per_s": round(world * seq["fp64_plain"], 3),
-                 "sequential_fp32_single_solves_per_s": round(world * seq["fp32_single"], 3),
-                 "speedup_vs_sequential_fp64": round(solves / wall / (world * seq["fp64_plain"]), 2),
-                 "sequential_sample": nseq,
+                 "sequential_fp64_plain_glups": round(s64u / 1e9, 3),
+                 "sequential_fp32_single_glups": round(world * seq["fp32_single"]["site_updates_per_s"] / 1e9, 3),
+                 "sequential_fp64_plain_solves_per_s_on_sample": round(world * seq["fp64_plain"]["solves_per_s"], 3),
+                 "speedup_vs_sequential_fp64": round(su / wall / s64u, 2),
+                 "speedup_basis": "site updates per second: the ensemble over the whole stream, the sequential "
+                                  "FP64 solves over requests spread evenly across it (including upload and "
+                                  "download of each solve)",
+                 "sequential_sample_request_ids": sample_ids,
+                 "accuracy": seq["accuracy"],
                  "stream": "Poisson 200 req/s, L log-uniform 16..96, steps 500..5000, g_br/g_bs/g_ss swept"}
+        rec = os.path.join(ROOT, "profiles", "serving_stream_4096.json")
+        if os.path.exists(rec):
+            with open(rec) as f:
+                serve["recorded_full_stream"] = json.load(f)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -414,18 +597,14 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded rho = 0.7 + U(-0.01,0.01) per component, unit dipoles",
-            "config": {"workload": f"ternary D3Q19 {L}^3 periodic, FP32-deviation storage",
-                       "lattice": [L, L, L], "g_br": 0.08, "g_bs": -0.006, "g_ss": -0.0045, "tau": 1.0,
-                       "tau_d": 1.0, "beta": 10.0, "parallelism": f"replicas x{world}",
-                       "l2": f"populations {2 * 57 * 4 * N / 1e6:.0f} MB > 126 MB L2, no flush",
-                       "launch_shape": list(shape[:3]),
-                       "strategy": ["fused", "split", "split, staged collide"][shape[3]],
-                       "shape_source": "fixed" if args.shape else "autotuned"},
+            "config": workload_config(world),
+            "path": {"storage": "FP32 deviations", "launch_shape": list(shape[:3]),
+                     "strategy": STRATEGIES[shape[3]], "shape_source": "fixed" if args.shape else "autotuned",
+                     "timed_blocks": nblocks, "block": f"{args.steps} steps, median block reported"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
-                         "traffic": (NCU_TRAFFIC_PER_SITE[(shape[0], shape[1], shape[3])] * N
-                                     if (shape[0], shape[1], shape[3]) in NCU_TRAFFIC_PER_SITE else None),
-                         "traffic_note": "DRAM bytes per step from one ncu capture of the three passes "
+                         "traffic": (ncu_traffic(shape) * N if ncu_traffic(shape) else None),
+                         "traffic_note": "DRAM bytes per step from one ncu capture of the step's passes "
                                          "(null for launch shapes without a capture)",
                          "peak_kind": peak_kind,
                          "bytes_per_site": BYTES_PER_SITE[("f32", 3)], "kernel_ms_per_step": round(per_step_ms, 4)},
