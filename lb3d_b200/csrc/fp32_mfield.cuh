@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
     const int x0 = T.x0, y0 = T.y0, z0 = T.z0, zc = T.zc;
     const int gx = x0 + tx, gy = y0 + ty;
     const bool act = gx < nx && gy < ny;
+    const bool le_edge = x0 == 0 || x0 + TX >= nx;  // the tile holds x = 0 or x = nx - 1
     // the ring of previous dipoles: plane z0 - 1 + j in slot j % DR
     auto load_db_plane = [&](int j) {
       const int gz = wrapz(z0 - 1 + j, nz);
@@ -216,8 +217,9 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
         for (int c = 0; c < NC; ++c) {
           float d[19];
           // Lees-Edwards lattices pull across x = 0 and x = nx - 1 from the
-          // sheared halo planes of this step
-          if constexpr (LE) {
+          // sheared halo planes of this step; tiles away from those planes
+          // pull as periodic lattices do
+          if (LE && le_edge) {
             pull_comp_le<NARROW>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
             le_store_boundary(Lg, 2, c, gx, gy, gz, d);  // for the stage-8 halo kernel
           } else {
@@ -450,75 +452,6 @@ __device__ __forceinline__ void force_ternary_pre(const float2 *Pm, const float2
   }
 }
 
-// Equilibrium deviations of one component written straight to the output
-// (full relaxation: the BGK update with omega = 1), with bgk_update's
-// arithmetic; out[q * S] receives population q.
-__device__ __forceinline__ void eq_store(float *out, unsigned S, float rho, float drho, float vx, float vy,
-                                         float vz, float omega) {
-  const float tx = 3.0f * vx, ty = 3.0f * vy, tz = 3.0f * vz;
-  const float uke = 0.5f * fmaf(tz, vz, fmaf(ty, vy, tx * vx));
-  const float a = -uke;
-  const float b = 1.0f + a;
-  const float orw = (omega * rho) * W1;
-  const float obase = (omega * drho) * W1;
-#define LB3D_EQ32(CD, I, J)                                               \
-  {                                                                       \
-    const float e = (CD);                                                 \
-    const float e2 = e * e;                                               \
-    const float ev = fmaf(orw, fmaf(0.5f, e2, a), obase);                 \
-    const float od = (orw * e) * fmaf(e2, 1.0f / 6.0f, b);                \
-    __stcs(out + (I) * S, ev + od);                                       \
-    __stcs(out + (J) * S, ev - od);                                       \
-  }
-  LB3D_EQ32(tx, 0, 1)
-  LB3D_EQ32(ty, 2, 3)
-  LB3D_EQ32(tz, 4, 5)
-  LB3D_EQ32(tx + ty, 6, 11)
-  LB3D_EQ32(tx - ty, 7, 10)
-  LB3D_EQ32(tx + tz, 8, 13)
-  LB3D_EQ32(tx - tz, 9, 12)
-  LB3D_EQ32(ty + tz, 14, 17)
-  LB3D_EQ32(ty - tz, 15, 16)
-#undef LB3D_EQ32
-  __stcs(out + 18 * S, fmaf((omega * rho) * W0, a, (omega * drho) * W0));
-}
-// eq_store for two components (lanes x, y) with bgk_update2's paired
-// arithmetic; lane x goes to outA, lane y to outB.
-__device__ __forceinline__ void eq_store2(float *outA, float *outB, unsigned S, float2 rho, float2 drho,
-                                          float2 vx, float2 vy, float2 vz, float2 omega) {
-  const float2 tx = mul2(f2(3.0f), vx), ty = mul2(f2(3.0f), vy), tz = mul2(f2(3.0f), vz);
-  const float2 uke = mul2(f2(0.5f), fma2(tz, vz, fma2(ty, vy, mul2(tx, vx))));
-  const float2 a = neg2(uke);
-  const float2 b = add2(f2(1.0f), a);
-  const float2 orw = mul2(mul2(omega, rho), f2(W1));
-  const float2 obase = mul2(mul2(omega, drho), f2(W1));
-#define LB3D_EQ2(CD, I, J)                                                    \
-  {                                                                           \
-    const float2 e = (CD);                                                    \
-    const float2 e2 = mul2(e, e);                                             \
-    const float2 ev = fma2(orw, fma2(f2(0.5f), e2, a), obase);                \
-    const float2 od = mul2(mul2(orw, e), fma2(e2, f2(1.0f / 6.0f), b));       \
-    const float2 p = add2(ev, od), m = add2(ev, neg2(od));                    \
-    __stcs(outA + (I) * S, p.x);                                              \
-    __stcs(outB + (I) * S, p.y);                                              \
-    __stcs(outA + (J) * S, m.x);                                              \
-    __stcs(outB + (J) * S, m.y);                                              \
-  }
-  LB3D_EQ2(tx, 0, 1)
-  LB3D_EQ2(ty, 2, 3)
-  LB3D_EQ2(tz, 4, 5)
-  LB3D_EQ2(add2(tx, ty), 6, 11)
-  LB3D_EQ2(add2(tx, neg2(ty)), 7, 10)
-  LB3D_EQ2(add2(tx, tz), 8, 13)
-  LB3D_EQ2(add2(tx, neg2(tz)), 9, 12)
-  LB3D_EQ2(add2(ty, tz), 14, 17)
-  LB3D_EQ2(add2(ty, neg2(tz)), 15, 16)
-#undef LB3D_EQ2
-  const float2 oeq0 = fma2(mul2(mul2(omega, rho), f2(W0)), a, mul2(mul2(omega, drho), f2(W0)));
-  __stcs(outA + 18 * S, oeq0.x);
-  __stcs(outB + 18 * S, oeq0.y);
-}
-
 // ---------------------------------------------------------------------------
 // Collide pass.  Plane m of a tile is field plane z0 - 1 + m (m = 0 ..
 // zc + 1).  Iteration j (0 .. zc + 2) waits for plane j, computes its psi
@@ -568,6 +501,7 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     const int npl = zc + 2;
     const int gx = x0 + tx, gy = y0 + ty;
     const bool act = gx < nx && gy < ny;
+    const bool le_edge = x0 == 0 || x0 + TX >= nx;  // the tile holds x = 0 or x = nx - 1
     auto issue = [&](int m) {
       const unsigned g = gbase + (unsigned)m;
       mf_issue(ring + (g % RS) * G::C_SLOT, G::BOX_BYTES, G::FIELD, &tm1, NC == 3 ? &tmd : nullptr, x0,
@@ -599,7 +533,7 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
       if (j < npl) {
         const float4 *M1 = box(g, 0);
         for (int s = tid; s < AN; s += NT) {
-          if constexpr (LE) {
+          if (LE && le_edge) {
             // the sheared halo columns take the psi deviations of the
             // stage-8 halo planes (binary lattices)
             const int vx = x0 - 1 + s % AW;
@@ -689,26 +623,29 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
             vz[c] = fmaf(kf, Fx[c][2], u2);
           }
           float *fo = Fo + self;
-          eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
-                    make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
-                    make_float2(Lg.omega[0], Lg.omega[1]));
+          if (LE && (gx == 0 || gx == nx - 1)) {
+            // a site on the sheared x boundary also writes the next step's
+            // pre-stream boundary plane for its stage-6 halo kernel (at
+            // x = 0 and x = nx - 1 both when the lattice is one site wide)
+            const int NP = ny * nz, o = gy + ny * gz;
+            float *b0 = Lg.le_b[gx == nx - 1 ? 0 : 1] + o;
+            eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+                      make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
+                      make_float2(Lg.omega[0], Lg.omega[1]), b0, b0 + 19 * NP, (unsigned)NP);
+            if (gx == 0 && gx == nx - 1) {
+              float *b1 = Lg.le_b[1] + o;
+              eq_store2(b1, b1 + 19 * NP, (unsigned)NP, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+                        make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
+                        make_float2(Lg.omega[0], Lg.omega[1]));
+            }
+          } else {
+            eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+                      make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
+                      make_float2(Lg.omega[0], Lg.omega[1]));
+          }
           if (NC == 3)
             eq_store(fo + (size_t)38 * S, S, rho[NC - 1], dr[NC - 1], vx[NC - 1], vy[NC - 1], vz[NC - 1],
                      Lg.omega[NC - 1]);
-          if constexpr (LE) {
-            // the next step's pre-stream populations of the x boundary
-            // planes, for its stage-6 halo kernel (read back from the
-            // thread's own stores)
-            if (gx == 0 || gx == nx - 1) {
-#pragma unroll
-              for (int c = 0; c < NC; ++c) {
-                float v[19];
-#pragma unroll
-                for (int q = 0; q < 19; ++q) v[q] = fo[(size_t)(c * 19 + q) * S];
-                le_store_boundary(Lg, 0, c, gx, gy, gz, v);
-              }
-            }
-          }
         }
       }
       op = op_next;

@@ -146,6 +146,88 @@ __device__ __forceinline__ void bgk_update2(float2 d[19], float2 rho, float2 drh
   d[18] = fma2(om1, d[18], oeq0);
 }
 
+// Equilibrium deviations of one component written straight to the output
+// (full relaxation: the BGK update with omega = 1), with bgk_update's
+// arithmetic; out[q * S] receives population q.
+__device__ __forceinline__ void eq_store(float *out, unsigned S, float rho, float drho, float vx, float vy,
+                                         float vz, float omega) {
+  const float tx = 3.0f * vx, ty = 3.0f * vy, tz = 3.0f * vz;
+  const float uke = 0.5f * fmaf(tz, vz, fmaf(ty, vy, tx * vx));
+  const float a = -uke;
+  const float b = 1.0f + a;
+  const float orw = (omega * rho) * W1;
+  const float obase = (omega * drho) * W1;
+#define LB3D_EQ32(CD, I, J)                                               \
+  {                                                                       \
+    const float e = (CD);                                                 \
+    const float e2 = e * e;                                               \
+    const float ev = fmaf(orw, fmaf(0.5f, e2, a), obase);                 \
+    const float od = (orw * e) * fmaf(e2, 1.0f / 6.0f, b);                \
+    __stcs(out + (I) * S, ev + od);                                       \
+    __stcs(out + (J) * S, ev - od);                                       \
+  }
+  LB3D_EQ32(tx, 0, 1)
+  LB3D_EQ32(ty, 2, 3)
+  LB3D_EQ32(tz, 4, 5)
+  LB3D_EQ32(tx + ty, 6, 11)
+  LB3D_EQ32(tx - ty, 7, 10)
+  LB3D_EQ32(tx + tz, 8, 13)
+  LB3D_EQ32(tx - tz, 9, 12)
+  LB3D_EQ32(ty + tz, 14, 17)
+  LB3D_EQ32(ty - tz, 15, 16)
+#undef LB3D_EQ32
+  __stcs(out + 18 * S, fmaf((omega * rho) * W0, a, (omega * drho) * W0));
+}
+// eq_store for two components (lanes x, y) with bgk_update2's paired
+// arithmetic; lane x goes to outA, lane y to outB.
+// With bA (optional) the two components' values also go to bA[q * SB] and
+// bB[q * SB].
+__device__ __forceinline__ void eq_store2(float *outA, float *outB, unsigned S, float2 rho, float2 drho,
+                                          float2 vx, float2 vy, float2 vz, float2 omega,
+                                          float *bA = nullptr, float *bB = nullptr, unsigned SB = 0) {
+  const float2 tx = mul2(f2(3.0f), vx), ty = mul2(f2(3.0f), vy), tz = mul2(f2(3.0f), vz);
+  const float2 uke = mul2(f2(0.5f), fma2(tz, vz, fma2(ty, vy, mul2(tx, vx))));
+  const float2 a = neg2(uke);
+  const float2 b = add2(f2(1.0f), a);
+  const float2 orw = mul2(mul2(omega, rho), f2(W1));
+  const float2 obase = mul2(mul2(omega, drho), f2(W1));
+#define LB3D_EQ2(CD, I, J)                                                    \
+  {                                                                           \
+    const float2 e = (CD);                                                    \
+    const float2 e2 = mul2(e, e);                                             \
+    const float2 ev = fma2(orw, fma2(f2(0.5f), e2, a), obase);                \
+    const float2 od = mul2(mul2(orw, e), fma2(e2, f2(1.0f / 6.0f), b));       \
+    const float2 p = add2(ev, od), m = add2(ev, neg2(od));                    \
+    __stcs(outA + (I) * S, p.x);                                              \
+    __stcs(outB + (I) * S, p.y);                                              \
+    __stcs(outA + (J) * S, m.x);                                              \
+    __stcs(outB + (J) * S, m.y);                                              \
+    if (bA) {                                                                 \
+      bA[(I) * SB] = p.x;                                                     \
+      bB[(I) * SB] = p.y;                                                     \
+      bA[(J) * SB] = m.x;                                                     \
+      bB[(J) * SB] = m.y;                                                     \
+    }                                                                         \
+  }
+  LB3D_EQ2(tx, 0, 1)
+  LB3D_EQ2(ty, 2, 3)
+  LB3D_EQ2(tz, 4, 5)
+  LB3D_EQ2(add2(tx, ty), 6, 11)
+  LB3D_EQ2(add2(tx, neg2(ty)), 7, 10)
+  LB3D_EQ2(add2(tx, tz), 8, 13)
+  LB3D_EQ2(add2(tx, neg2(tz)), 9, 12)
+  LB3D_EQ2(add2(ty, tz), 14, 17)
+  LB3D_EQ2(add2(ty, neg2(tz)), 15, 16)
+#undef LB3D_EQ2
+  const float2 oeq0 = fma2(mul2(mul2(omega, rho), f2(W0)), a, mul2(mul2(omega, drho), f2(W0)));
+  __stcs(outA + 18 * S, oeq0.x);
+  __stcs(outB + 18 * S, oeq0.y);
+  if (bA) {
+    bA[18 * SB] = oeq0.x;
+    bB[18 * SB] = oeq0.y;
+  }
+}
+
 // Own-site moments of one component's post-stream deviations d[q * ST]:
 // drho = sum_q g_q d_q and j = sum_q g_q c_q d_q, in q order, one fused
 // multiply-add per term.

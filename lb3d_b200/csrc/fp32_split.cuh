@@ -219,11 +219,19 @@ __global__ void __launch_bounds__(TX *TY, 768 / (TX * TY))
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
               const float k = Lg.tau[c] / (Lg.amass[c] * fmaxf(rho[c], 1.0e-8f));
+              float *fo = Fo + (size_t)(c * 19) * S + self;
+              if (Lg.omega[c] == 1.0f) {
+                // full relaxation: the BGK update is the equilibrium, the
+                // populations drop out and need no pull (the own moments
+                // came from the moments pass)
+                eq_store(fo, S, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
+                         fmaf(k, Fx[c][2], u2), Lg.omega[c]);
+                continue;
+              }
               float d[19];
               pull_comp<ROCK, true>(F, S, c, nb, self, RK, d);
               bgk_update(d, rho[c], dr[c], fmaf(k, Fx[c][0], u0), fmaf(k, Fx[c][1], u1),
                          fmaf(k, Fx[c][2], u2), Lg.omega[c]);
-              float *fo = Fo + (size_t)(c * 19) * S + self;
 #pragma unroll
               for (int q = 0; q < 19; ++q) __stcs(fo + q * S, d[q]);
             }
