@@ -206,6 +206,17 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
         // (the force stencil takes the rock colour there): no pulls
         if (ROCK) fluid = __ldg(rock + self) == 0;
       }
+      if (LE && ROCK && act && !fluid && le_edge) {
+        // a rock site on the sheared boundary keeps its (zero) populations:
+        // they go to the post-stream boundary plane as they are
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          float d[19];
+#pragma unroll
+          for (int q = 0; q < 19; ++q) d[q] = __ldg(F + (size_t)(c * 19 + q) * S + self);
+          le_store_boundary(Lg, 2, c, gx, gy, gz, d);
+        }
+      }
       if (fluid) {
         float dr[NC], jm[NC][3];
         float a0 = 0.f, a1 = 0.f, a2 = 0.f;
@@ -220,7 +231,7 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
           // sheared halo planes of this step; tiles away from those planes
           // pull as periodic lattices do
           if (LE && le_edge) {
-            pull_comp_le<NARROW>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
+            pull_comp_le<NARROW, ROCK>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d, rock);
             le_store_boundary(Lg, 2, c, gx, gy, gz, d);  // for the stage-8 halo kernel
           } else {
             pull_comp<ROCK, false, NARROW>(F, S, c, nb, self, rock, d);
@@ -573,9 +584,9 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
                                   dnow, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
           } else {
             const float2 *P2 = reinterpret_cast<const float2 *>(psiring);
-            force_binary<AW, ROCK>(P2 + ((mc + PR - 1) % PR) * AN, P2 + (mc % PR) * AN,
-                                   P2 + ((mc + 1) % PR) * AN, ap, nb, rock, Lg, psi0,
-                                   reinterpret_cast<float(*)[3]>(Fx));
+            force_binary<AW, ROCK, float2, LE>(P2 + ((mc + PR - 1) % PR) * AN, P2 + (mc % PR) * AN,
+                                               P2 + ((mc + 1) % PR) * AN, ap, nb, rock, Lg, psi0,
+                                               reinterpret_cast<float(*)[3]>(Fx), gx, gy, gz);
           }
           // own densities and weighted momentum
           const float4 o1 = box(gc, 0)[ap];

@@ -352,21 +352,28 @@ __device__ __forceinline__ void make_leyz(LeYZ &w, int gy, int gz, int ny, int n
   w.z[1] = ny * gz;
   w.z[2] = ny * (gz == nz - 1 ? 0 : gz + 1);
 }
-template <int Q>
+// With ROCK (walls) the sheared halo sites are never rock, as the
+// reference's exchange leaves them (code/lb3d_bc_leesedwards.F90:678,866),
+// and a pull from a rock site inside the lattice bounces back.
+template <int Q, bool ROCK = false>
 __device__ __forceinline__ const float *le_src(const float *fc, unsigned S, int c, const Nbr &n, int gx,
-                                               int nx, const LeYZ &w, const LatDesc &Lg, int NP) {
+                                               int nx, const LeYZ &w, const LatDesc &Lg, int NP,
+                                               int self = 0, const uint8_t *__restrict__ rk = nullptr) {
   if (cx(Q) == 1 && gx == 0) return Lg.le_h[0] + (c * 19 + Q) * NP + w.y[1 - cy(Q)] + w.z[1 - cz(Q)];
   if (cx(Q) == -1 && gx == nx - 1)
     return Lg.le_h[1] + (c * 19 + Q) * NP + w.y[1 - cy(Q)] + w.z[1 - cz(Q)];
-  return fc + Q * S + noff<Q, -1>(n);
+  const int up = noff<Q, -1>(n);
+  if (ROCK && __ldg(rk + up) != 0) return fc + bounce(Q) * S + self;
+  return fc + Q * S + up;
 }
-template <bool NARROW = false>
+template <bool NARROW = false, bool ROCK = false>
 __device__ __forceinline__ void pull_comp_le(const float *__restrict__ F, unsigned S, int c, const Nbr &n,
                                              int self, int gx, int nx, const LeYZ &w,
-                                             const LatDesc &Lg, int NP, float d[19]) {
+                                             const LatDesc &Lg, int NP, float d[19],
+                                             const uint8_t *__restrict__ rk = nullptr) {
   const float *fc = NARROW ? F + (unsigned)(c * 19) * S : F + (size_t)(c * 19) * S;
   d[18] = __ldg(fc + 18 * S + self);
-#define LB3D_PULL_LE(Q) d[Q] = __ldg(le_src<Q>(fc, S, c, n, gx, nx, w, Lg, NP));
+#define LB3D_PULL_LE(Q) d[Q] = __ldg(le_src<Q, ROCK>(fc, S, c, n, gx, nx, w, Lg, NP, self, rk));
   LB3D_PULL_LE(0) LB3D_PULL_LE(1) LB3D_PULL_LE(2) LB3D_PULL_LE(3) LB3D_PULL_LE(4) LB3D_PULL_LE(5)
   LB3D_PULL_LE(6) LB3D_PULL_LE(7) LB3D_PULL_LE(8) LB3D_PULL_LE(9) LB3D_PULL_LE(10) LB3D_PULL_LE(11)
   LB3D_PULL_LE(12) LB3D_PULL_LE(13) LB3D_PULL_LE(14) LB3D_PULL_LE(15) LB3D_PULL_LE(16) LB3D_PULL_LE(17)
@@ -568,7 +575,15 @@ __global__ void __launch_bounds__(TX *TY, (MODE == MODE_MOMENTS ? 1024 / (TX * T
           for (int c = 0; c < NC; ++c) {
             float d[19];
             if constexpr (LE) {
-              pull_comp_le<NARROW>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d);
+              if (ROCK && __ldg(RK + self) != 0) {
+                // a rock site keeps its (zero) populations
+                // (code/lb3d_advection.F90:109-151 pulls into fluid sites only)
+                const float *fc = F + (size_t)(c * 19) * S + self;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) d[q] = __ldg(fc + q * S);
+              } else {
+                pull_comp_le<NARROW, ROCK>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, d, RK);
+              }
               // the post-stream populations of the x boundary planes, for
               // the stage-8 halo kernel
               if (MODE == MODE_MOMENTS && x0 + ax < nx && y0 + ay < ny)
@@ -913,8 +928,12 @@ static const void *mode_fn(int nc, bool rock, bool body, const FusedShape &sh) {
   if constexpr (LE) {
     static_assert(MODE == MODE_MOMENTS || MODE == MODE_MOMENTS32 || MODE == MODE_COLLIDE2,
                   "no Lees-Edwards variant");
-    if (nc != 2 || rock) return nullptr;
-    if (body) { LB3D_SHAPES(2, false, true) } else { LB3D_SHAPES(2, false, false) }
+    if (nc != 2) return nullptr;
+    if (rock) {
+      if (body) { LB3D_SHAPES(2, true, true) } else { LB3D_SHAPES(2, true, false) }
+    } else {
+      if (body) { LB3D_SHAPES(2, false, true) } else { LB3D_SHAPES(2, false, false) }
+    }
     return nullptr;
   }
   if (MODE == MODE_DIPOLE) rock = false;
@@ -1046,7 +1065,7 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
   const unsigned S = (unsigned)S64;
   if (le) {
     // stage 6 halo, moments pass, stage 8 halo, staged collide pass
-    if (!P || nc != 2 || rock || sh.split != 2 || !M) return cudaErrorInvalidValue;
+    if (!P || nc != 2 || sh.split != 2 || !M) return cudaErrorInvalidValue;
     // one thread per (y, z) of the x-halo planes: 64-thread blocks spread
     // the few thousand threads over every SM
     const unsigned g = (unsigned)((P->ny * P->nz + 63) / 64);
@@ -1264,8 +1283,12 @@ static bool mf_fns(int nc, bool rock, bool body, int tx, int ty, bool narrow, co
   if (tx == 16 && ty == 8) return mf_ptrs<NC, 16, 8, R, B, L>(narrow, mom, dip, col), true;   \
   if (tx == 64 && ty == 4) return mf_ptrs<NC, 64, 4, R, B, L>(narrow, mom, dip, col), true;
   if (le) {
-    if (nc != 2 || rock) return false;
-    if (body) { LB3D_MF(2, false, true, true) } else { LB3D_MF(2, false, false, true) }
+    if (nc != 2) return false;
+    if (rock) {
+      if (body) { LB3D_MF(2, true, true, true) } else { LB3D_MF(2, true, false, true) }
+    } else {
+      if (body) { LB3D_MF(2, false, true, true) } else { LB3D_MF(2, false, false, true) }
+    }
     return false;
   }
   if (nc == 3) {
@@ -1689,7 +1712,6 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   // the caller has uploaded the rock flags (rockp, device) and set any_rock
   const bool any = P.any_rock != 0;
   if (any && P.nc == 3) return LB3DC_EINVAL;
-  if (any && P.le) return LB3DC_ENOTSUP;  // the FP32 Lees-Edwards kernels have no walls
   s.lat = fp32_make_desc(P, rho0, 0, any);
   attach_le(s);
   s.lat.parity = 0;

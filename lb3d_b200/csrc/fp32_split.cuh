@@ -300,14 +300,16 @@ __device__ __forceinline__ void pull_async(const float *__restrict__ F, unsigned
 #undef LB3D_APULL
 }
 
-// pull_async with the Lees-Edwards halo planes across the x boundary
-template <int NT>
+// pull_async with the Lees-Edwards halo planes across the x boundary (with
+// ROCK: bounce-back from rock sites inside the lattice, as le_src)
+template <int NT, bool ROCK = false>
 __device__ __forceinline__ void pull_async_le(const float *__restrict__ F, unsigned S, int c, const Nbr &n,
                                               int self, int gx, int nx, const LeYZ &w,
-                                              const LatDesc &Lg, int NP, float *stage) {
+                                              const LatDesc &Lg, int NP, float *stage,
+                                              const uint8_t *__restrict__ rk = nullptr) {
   const float *fc = F + (size_t)(c * 19) * S;
   cp_async4(stage + 18 * NT, fc + 18 * S + self);
-#define LB3D_APULL_LE(Q) cp_async4(stage + (Q) * NT, le_src<Q>(fc, S, c, n, gx, nx, w, Lg, NP));
+#define LB3D_APULL_LE(Q) cp_async4(stage + (Q) * NT, le_src<Q, ROCK>(fc, S, c, n, gx, nx, w, Lg, NP, self, rk));
   LB3D_APULL_LE(0) LB3D_APULL_LE(1) LB3D_APULL_LE(2) LB3D_APULL_LE(3) LB3D_APULL_LE(4)
   LB3D_APULL_LE(5) LB3D_APULL_LE(6) LB3D_APULL_LE(7) LB3D_APULL_LE(8) LB3D_APULL_LE(9)
   LB3D_APULL_LE(10) LB3D_APULL_LE(11) LB3D_APULL_LE(12) LB3D_APULL_LE(13) LB3D_APULL_LE(14)
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
         make_leyz(lw, gy, gz, ny, nz);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
-          pull_async_le<NT>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, mystage + c * 19 * NT);
+          pull_async_le<NT, ROCK>(F, S, c, nb, self, gx, nx, lw, Lg, ny * nz, mystage + c * 19 * NT, RK);
       } else {
 #pragma unroll
         for (int c = 0; c < NC; ++c) pull_async<ROCK, NT>(F, S, c, nb, self, RK, mystage + c * 19 * NT);
@@ -437,7 +439,8 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
           // binary rings hold {dpsi_r, dpsi_b}
           const float2 *Qm = ringP2 + (k % RS) * AN, *Q0 = ringP2 + ((k + 1) % RS) * AN,
                        *Qp = ringP2 + ((k + 2) % RS) * AN;
-          force_binary<AW, ROCK>(Qm, Q0, Qp, as, nb, RK, Lg, psi0, reinterpret_cast<float(*)[3]>(Fx));
+          force_binary<AW, ROCK, float2, LE>(Qm, Q0, Qp, as, nb, RK, Lg, psi0,
+                                             reinterpret_cast<float(*)[3]>(Fx), gx, gy, gzc);
         }
       }
       cp_async_wait<1>();  // this thread's pulls of plane k landed

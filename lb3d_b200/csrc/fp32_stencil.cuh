@@ -157,10 +157,16 @@ __device__ __forceinline__ void force_ternary(const float4 *Pm, const float4 *P0
 }
 
 // Binary force with walls (:127-210) from psi entries {dpsi_r, dpsi_b, -, -}.
-template <int W, bool ROCK, typename E>
+// LE (a Lees-Edwards lattice; the site at gx, gy, gz): a neighbour across the
+// sheared x boundary is a halo site, never rock; a rock neighbour reached
+// through the periodic y or z wrap has no rock colour there, as the
+// reference's y and z exchanges of a sheared lattice leave it
+// (code/lb3d_bc_leesedwards.F90:1079-1308): psi(0) = 0 on the wall side.
+template <int W, bool ROCK, typename E, bool LE = false>
 __device__ __forceinline__ void force_binary(const E *Pm, const E *P0, const E *Pp,
                                              int as, const Nbr &nb, const uint8_t *__restrict__ RK,
-                                             const LatDesc &Lg, float psi0, float Fx[2][3]) {
+                                             const LatDesc &Lg, float psi0, float Fx[2][3], int gx = 0,
+                                             int gy = 0, int gz = 0) {
   float frb[3] = {0, 0, 0}, fbr[3] = {0, 0, 0}, fwr[3] = {0, 0, 0}, fwb[3] = {0, 0, 0};
 #pragma unroll
   for (int q = 0; q < 18; ++q) {
@@ -168,8 +174,13 @@ __device__ __forceinline__ void force_binary(const E *Pm, const E *P0, const E *
     const int an = as + cx(q) + W * cy(q);
     const float g = (float)gw(q);
     const int c[3] = {cx(q), cy(q), cz(q)};
-    bool nrock = false;
-    if (ROCK) nrock = __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
+    bool nrock = false, colour = true;
+    if (ROCK) {
+      const bool xhalo = LE && (gx + cx(q) < 0 || gx + cx(q) >= Lg.nx);
+      nrock = !xhalo && __ldg(RK + nb.cx[1 + cx(q)] + nb.ry[1 + cy(q)] + nb.rz[1 + cz(q)]) != 0;
+      if (LE && nrock)
+        colour = !(gy + cy(q) < 0 || gy + cy(q) >= Lg.ny || gz + cz(q) < 0 || gz + cz(q) >= Lg.nz);
+    }
     const E e = Pq[an];
     const float pr = nrock ? -psi0 : e.x, pb = nrock ? -psi0 : e.y;
 #pragma unroll
@@ -177,7 +188,7 @@ __device__ __forceinline__ void force_binary(const E *Pm, const E *P0, const E *
       if (c[k]) {
         frb[k] = fmaf(pb * g, (float)c[k], frb[k]);
         fbr[k] = fmaf(pr * g, (float)c[k], fbr[k]);
-        if (ROCK && nrock) {
+        if (ROCK && nrock && colour) {
           fwb[k] = fmaf(Lg.psiw_b * g, (float)c[k], fwb[k]);
           fwr[k] = fmaf(Lg.psiw_r * g, (float)c[k], fwr[k]);
         }

@@ -176,19 +176,66 @@ def test_fp32_lees_edwards_offsets(dims, shear_u, omega):
 
 
 def test_fp32_lees_edwards_limits():
-    """The FP32 Lees-Edwards kernels have no walls and exist for the staged
-    split strategy only; both limits are reported, not run."""
+    """The FP32 Lees-Edwards kernels exist for the staged split strategy and
+    the moment-field strategy only; the others are refused."""
     from lb3d_b200.lib import Lattice, Lb3dError
     p = _params((16, 8, 8), 2, boundary_cond=-1, inv_fluid=5, shear_u=0.05)
     st = uniform_mixture(16, 8, 8, 2, seed=1)
     lat = Lattice(p, precision=1)
     lat.upload_state(st)
-    with pytest.raises(Lb3dError):
-        lat.set_launch_shape(32, 8, 16, 1)
-    st["rock"] = np.zeros((8, 8, 16))
-    st["rock"][0, 0, 0] = 1.0
-    with pytest.raises(Lb3dError):
-        Lattice(p, precision=1).upload_state(st)
+    for split in (0, 1):
+        with pytest.raises(Lb3dError):
+            lat.set_launch_shape(32, 8, 16, split)
+
+
+@pytest.mark.parametrize("shear_u,omega", [(0.05, 0.0), (-0.3, 0.0), (0.2, 0.31)])
+@pytest.mark.parametrize("split", [2, 3])
+def test_fp32_lees_edwards_with_walls(split, shear_u, omega):
+    """Binary Lees-Edwards with rock (legal in the reference): rock inside, a
+    wall on the first z plane (met through the periodic z wrap, where the
+    reference's sheared exchange drops the rock colour) and rock on the
+    sheared x planes, whose halo sites are never rock.  Against the FP64
+    oracle within the FP32 tolerances, for both strategies that run
+    Lees-Edwards lattices."""
+    from lb3d_b200.lib import Lattice
+    dims = (8, 6, 10)
+    p = _params(dims, 2, boundary_cond=-1, inv_fluid=5, shear_u=shear_u, shear_omega=omega,
+                g_wr=-0.05, g_wb=0.03, rock_colour_r=0.7, rock_colour_b=0.4)
+    st = uniform_mixture(*dims, 2, seed=5)
+    rock = np.zeros(dims[::-1])
+    rock[0, :, 3:5] = 1.0
+    rock[4, 2, 0] = 1.0
+    rock[6, 3, 7] = 1.0
+    rock[5, 1, 5] = 1.0
+    st["rock"] = rock
+    st["shear_sum"] = 0.37
+    lat = Lattice(p, precision=1)
+    lat.upload_state(st)
+    lat.set_launch_shape(16, 8, 16, split)
+    o = Oracle(p, st)
+    for _ in range(2):
+        lat.time_loop(10)
+        o.run(10)
+        check(lat.download(), o.get(), 2, f"LE+rock strategy {split} shear_u={shear_u}")
+    assert lat.lees_edwards[0] == o.shear_sum
+
+
+def test_fp32_lees_edwards_with_walls_strategies_agree():
+    from lb3d_b200.lib import Lattice
+    dims = (40, 12, 20)
+    p = _params(dims, 2, boundary_cond=-1, inv_fluid=5, shear_u=-0.3, g_wr=-0.1, g_wb=0.05,
+                rock_colour_r=1.0, rock_colour_b=0.5, g_accn_x=1e-5)
+    st = uniform_mixture(*dims, 2, seed=9)
+    rng = np.random.default_rng(4)
+    st["rock"] = (rng.random(dims[::-1]) < 0.15).astype(np.float64)
+    out = []
+    for split in (2, 3):
+        lat = Lattice(p, precision=1)
+        lat.upload_state(st)
+        lat.set_launch_shape(32, 4, 16, split)
+        lat.time_loop(15)
+        out.append(lat.download())
+    assert np.array_equal(out[0]["n"], out[1]["n"])
 
 
 def test_fp32_sanity_velocity_and_sums_on_device():
