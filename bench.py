@@ -392,8 +392,9 @@ def run_accuracy(args):
     velocity), plus one statistical observable per workload (the first
     moment of the order parameter's structure factor and the L1 distance of
     its histogram for the phase-separating mixtures, the Darcy flux for the
-    porous one).  A mixed (non-phase-separating) ternary lattice is added,
-    where the pointwise bound can hold for any number of steps.  The FP64
+    porous one).  Two lattices below the demixing threshold are added: a
+    binary one (g_br 0.02), where the pointwise bound holds, and a ternary
+    one (g_br 0.01), whose surfactant still forms a lattice-scale pattern.  The FP64
     path is bit-identical to the oracle, so it stands in for it here."""
     import torch
     from lb3d_b200.config import Params
@@ -405,6 +406,9 @@ def run_accuracy(args):
     if "ternary-128" in args.accuracy_cases:
         cases.append(("ternary-128", workload_params(precision=0), lambda: uniform_mixture(L, L, L, 3, seed=1),
                       [1000, 10000]))
+    if "binary-64-mixed" in args.accuracy_cases:
+        pb = Params(nx=64, ny=64, nz=64, ncomp=2, **{**phys2, "g_br": 0.02}).finalize()
+        cases.append(("binary-64-mixed", pb, lambda: uniform_mixture(64, 64, 64, 2, seed=5), [1000, 10000]))
     if "mixed-64" in args.accuracy_cases:
         pm = Params(nx=64, ny=64, nz=64, ncomp=3, **{**PHYS, "g_br": args.mixed_g_br}).finalize()
         cases.append(("ternary-64-mixed", pm, lambda: uniform_mixture(64, 64, 64, 3, seed=2), [1000, 10000]))
@@ -483,8 +487,9 @@ def main():
                     "Lees-Edwards 256x128x128, porous 256^3) instead")
     ap.add_argument("--accuracy", action="store_true", help="FP32 vs FP64 error and the FP64 sensitivity "
                     "floor on the benchmark workloads, with statistical observables")
-    ap.add_argument("--accuracy-cases", default="ternary-128,mixed-64,lees-edwards,porous")
-    ap.add_argument("--mixed-g-br", type=float, default=0.005)
+    ap.add_argument("--accuracy-cases",
+                    default="ternary-128,mixed-64,binary-64-mixed,lees-edwards,porous")
+    ap.add_argument("--mixed-g-br", type=float, default=0.01)
     ap.add_argument("--shape", default=None,
                     help="tx,ty,zc,split: fixed FP32 launch shape instead of the autotuner (profiling runs)")
     args = ap.parse_args()

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/lb3dc.h"
@@ -254,6 +255,15 @@ int need_loaded(lb3dc_handle *h) {
   if (!h->loaded) return fail(h, LB3DC_ESTATE, "no state loaded (call lb3dc_upload_state first)");
   cudaSetDevice(h->device);
   return LB3DC_OK;
+}
+
+// The FP64 time loop streams inside the collision (fp64_step_pull) unless
+// something runs between the two: the Lees-Edwards stage-8 halo or an
+// invasion boundary on the post-stream populations.
+bool fp64_pull_ok(const lb3dc_handle *h) {
+  if (h->p.precision != LB3DC_FP64 || h->le || h->P.zouhe) return false;
+  const int k = h->p.inv_fluid;
+  return !(h->p.boundary_cond != 0 && (k == 11 || k == 7 || k == 8));
 }
 
 int ensure_scratch(lb3dc_handle *h, long long bytes) {
@@ -566,7 +576,7 @@ int lb3dc_advection(lb3dc_handle *h) {
     CK(h, fp64_stream(h->P, h->f, h->g, h->rho, h->psi, h->mom, h->da, h->db, h->rock, h->hlo,
                       h->hhi, h->stream));
     h->timer.stop(h->stream);
-    h->timer.launches += 1;
+    h->timer.launches += h->P.nc;
   } else {
     // The FP32 path streams inside its fused stream-collide kernel.
     h->pending_advection = true;
@@ -607,6 +617,21 @@ int lb3dc_time_loop(lb3dc_handle *h, int nsteps) {
     h->nt += nsteps;
     rc = fp32_run(h->P, h->s32, h->rock, nsteps, h->stream);
     if (rc) return fail(h, LB3DC_ECUDA, "FP32 run failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return LB3DC_OK;
+  }
+  if (fp64_pull_ok(h)) {
+    // stages 6 and 8 have nothing to do here; each step is the moments
+    // pass, the dipole relaxation and the pulling collision, f -> g, after
+    // which f and g trade places
+    for (int s = 0; s < nsteps; ++s) {
+      h->nt += 1;
+      h->timer.start(h->stream);
+      CK(h, fp64_step_pull(h->P, h->f, h->g, h->rho, h->psi, h->mom, h->da, h->db, h->rock,
+                           h->stream));
+      h->timer.stop(h->stream);
+      h->timer.launches += h->P.nc + (h->p.ncomp == 3 ? 1 : 0) + 1;
+      std::swap(h->f, h->g);
+    }
     return LB3DC_OK;
   }
   for (int s = 0; s < nsteps; ++s) {

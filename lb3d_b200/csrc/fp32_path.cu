@@ -1643,8 +1643,11 @@ int fp32_alloc(const DevParams &P, const lb3dc_params &p, Fp32State &s, cudaStre
   if (cudaMalloc(&s.M, (size_t)N * fp32_moment_bytes(P.nc)) != cudaSuccess) return LB3DC_ENOMEM;
   s.bytes += N * fp32_moment_bytes(P.nc);
   if (cudaMalloc(&s.d_lat, sizeof(LatDesc)) != cudaSuccess) return LB3DC_ENOMEM;
-  if (cudaMalloc(&s.stage, (size_t)N * sizeof(double)) != cudaSuccess) return LB3DC_ENOMEM;
-  s.bytes += N * (long long)sizeof(double);
+  if (cudaMalloc(&s.stage, 2 * (size_t)N * sizeof(double)) != cudaSuccess) return LB3DC_ENOMEM;
+  s.bytes += 2 * N * (long long)sizeof(double);
+  if (cudaStreamCreateWithFlags(&s.xs, cudaStreamNonBlocking) != cudaSuccess) return LB3DC_ECUDA;
+  for (int i = 0; i < 4; ++i)
+    if (cudaEventCreateWithFlags(&s.xev[i], cudaEventDisableTiming) != cudaSuccess) return LB3DC_ECUDA;
   if (P.le) {
     const size_t np = (size_t)P.ny * P.nz;
     for (int b = 0; b < 2; ++b) {
@@ -1689,6 +1692,12 @@ void fp32_free(Fp32State &s) {
   s.mf_tx = s.mf_ty = 0;
   if (s.stage) cudaFree(s.stage);
   s.stage = nullptr;
+  for (int i = 0; i < 4; ++i) {
+    if (s.xev[i]) cudaEventDestroy(s.xev[i]);
+    s.xev[i] = nullptr;
+  }
+  if (s.xs) cudaStreamDestroy(s.xs);
+  s.xs = nullptr;
   for (int b = 0; b < 2; ++b) {
     if (s.le_h[b]) cudaFree(s.le_h[b]);
     if (s.le_p[b]) cudaFree(s.le_p[b]);
@@ -1715,22 +1724,33 @@ int fp32_upload(const DevParams &P, const lb3dc_params &p, Fp32State &s, const d
   s.lat = fp32_make_desc(P, rho0, 0, any);
   attach_le(s);
   s.lat.parity = 0;
-  // one FP64 plane at a time through the staging buffer: populations
-  // converted to deviations, dipoles rounded to FP32, into both buffers
-  cudaError_t e = cudaSuccess;
+  // one FP64 plane at a time through two staging planes: the copy of plane
+  // cq + 1 (copy stream) overlaps the conversion of plane cq (populations to
+  // deviations, dipoles rounded to FP32, into both buffers); xev[b] marks
+  // staging plane b filled, xev[2 + b] drained
   const int nplanes = P.nc * 19 + (P.nc == 3 ? 3 : 0);
+  cudaError_t e = cudaEventRecord(s.xev[2], st);
+  if (e == cudaSuccess) e = cudaEventRecord(s.xev[3], st);
   for (int cq = 0; cq < nplanes && e == cudaSuccess; ++cq) {
+    const int b = cq & 1;
+    double *stg = s.stage + (size_t)b * N;
     const bool pop = cq < P.nc * 19;
     const double *src = pop ? n + (size_t)cq * N : db + (size_t)(cq - P.nc * 19) * N;
     float *d0 = pop ? s.f[0] + (size_t)cq * s.S : s.db[0] + (size_t)(cq - P.nc * 19) * s.S;
     float *d1 = pop ? s.f[1] + (size_t)cq * s.S : s.db[1] + (size_t)(cq - P.nc * 19) * s.S;
     const double w = pop ? (cq % 19 == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0 : 0.0;
-    e = cudaMemcpyAsync(s.stage, src, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, st);
+    e = cudaStreamWaitEvent(s.xs, s.xev[2 + b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(stg, src, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s.xs);
+    if (e == cudaSuccess) e = cudaEventRecord(s.xev[b], s.xs);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, s.xev[b], 0);
     if (e != cudaSuccess) break;
-    k_plane_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.stage, d0, d1, N, w,
+    k_plane_from_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(stg, d0, d1, N, w,
                                                                     any ? rockp : nullptr);
     e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(s.xev[2 + b], st);
   }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s.xs);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return LB3DC_ECUDA;
   if (cudaMemcpyAsync(s.d_lat, &s.lat, sizeof(LatDesc), cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -1757,17 +1777,29 @@ int fp32_download(const DevParams &P, const lb3dc_params &p, Fp32State &s, doubl
     nn = tmp.data();
   }
   if (nn) {
-    // deviations -> FP64 populations, one plane at a time through the staging buffer
-    cudaError_t e = cudaSuccess;
+    // deviations -> FP64 populations, one plane at a time through two
+    // staging planes: the conversion of plane cq + 1 overlaps the copy of
+    // plane cq (copy stream); xev[b] marks staging plane b filled, xev[2 + b]
+    // drained
+    cudaError_t e = cudaEventRecord(s.xev[2], s.xs);
+    if (e == cudaSuccess) e = cudaEventRecord(s.xev[3], s.xs);
     for (int cq = 0; cq < nc * 19 && e == cudaSuccess; ++cq) {
+      const int b = cq & 1;
+      double *stg = s.stage + (size_t)b * N;
       const double w = (cq % 19 == 18 ? 1.0 / 3.0 : 1.0 / 36.0) * rho0;
+      e = cudaStreamWaitEvent(st, s.xev[2 + b], 0);
+      if (e != cudaSuccess) break;
       k_plane_to_fp64<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(s.f[cur] + (size_t)cq * s.S,
-                                                                    s.stage, N, w);
+                                                                    stg, N, w);
       e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaEventRecord(s.xev[b], st);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s.xs, s.xev[b], 0);
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(nn + (size_t)cq * N, s.stage, (size_t)N * sizeof(double),
-                            cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(nn + (size_t)cq * N, stg, (size_t)N * sizeof(double),
+                            cudaMemcpyDeviceToHost, s.xs);
+      if (e == cudaSuccess) e = cudaEventRecord(s.xev[2 + b], s.xs);
     }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.xs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return LB3DC_ECUDA;
   }

@@ -68,7 +68,11 @@ struct Fp32State {
   int grid = 0;
   long long bytes = 0;
   KernelTimer *timer = nullptr;  // optional, owned by the handle
-  double *stage = nullptr;  // one FP64 population plane (N sites) for uploads and downloads
+  // two FP64 population planes (N sites each) for uploads and downloads: the
+  // copy of one plane on the copy stream overlaps the conversion of the other
+  double *stage = nullptr;
+  cudaStream_t xs = nullptr;                         // copy stream
+  cudaEvent_t xev[4] = {nullptr, nullptr, nullptr, nullptr};  // per plane: filled, drained
   float *le_h[2] = {nullptr, nullptr};  // Lees-Edwards halo planes (see LatDesc)
   float2 *le_p[2] = {nullptr, nullptr};
   float *le_b[4] = {nullptr, nullptr, nullptr, nullptr};

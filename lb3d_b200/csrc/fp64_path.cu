@@ -103,8 +103,10 @@ __global__ void k_le_halo(DevParams P, LEStep S, const double *__restrict__ src,
 // One launch per component c (components are independent here; the
 // advected dipole flux uses the surfactant only), which keeps one
 // component's 19 pulls live per thread; FLUX marks the surfactant launch,
-// which also accumulates the dipole flux.
-template <int NC, bool LE, bool FLUX, bool ROCK>
+// which also accumulates the dipole flux.  STORE writes the post-stream
+// populations to fout and MOM the momenta: the moments pass of the pulling
+// step (k_collide with PULL) writes the moments only.
+template <int NC, bool LE, bool FLUX, bool ROCK, bool STORE = true, bool MOM = true>
 __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__restrict__ fin,
                                                 double *__restrict__ fout, double *__restrict__ rho,
                                                 double *__restrict__ psi, double *__restrict__ mom,
@@ -198,21 +200,23 @@ __global__ void __launch_bounds__(256, 2) k_stream(DevParams P, const double *__
     double r = 0.0, u0 = 0.0, u1 = 0.0, u2 = 0.0;
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
-      fout[(c * 19 + q) * N + i] = n[q];
+      if (STORE) fout[(c * 19 + q) * N + i] = n[q];
       r = r + n[q] * (double)gw(q);
-    }
-#pragma unroll
-    for (int q = 0; q < 19; ++q) {
-      double ng = n[q] * (double)gw(q);
-      u0 = u0 + ng * (double)cx(q);
-      u1 = u1 + ng * (double)cy(q);
-      u2 = u2 + ng * (double)cz(q);
     }
     rho[c * N + i] = r;
     psi[c * N + i] = get_psi(r);
-    mom[(c * 3 + 0) * N + i] = u0;
-    mom[(c * 3 + 1) * N + i] = u1;
-    mom[(c * 3 + 2) * N + i] = u2;
+    if (MOM) {
+#pragma unroll
+      for (int q = 0; q < 19; ++q) {
+        double ng = n[q] * (double)gw(q);
+        u0 = u0 + ng * (double)cx(q);
+        u1 = u1 + ng * (double)cy(q);
+        u2 = u2 + ng * (double)cz(q);
+      }
+      mom[(c * 3 + 0) * N + i] = u0;
+      mom[(c * 3 + 1) * N + i] = u1;
+      mom[(c * 3 + 2) * N + i] = u2;
+    }
   }
   if (FLUX) {
     da[i] = d0;
@@ -506,10 +510,17 @@ __device__ __forceinline__ void sc_forces(const DevParams &P, int x, int y, int 
 }
 
 // ---------------------------------------------------------------------------
-// Forces + BGK, code/lb3d_collision.F90:151-289.
+// Forces + BGK, code/lb3d_collision.F90:151-289.  With PULL (periodic
+// lattices without stage-8 boundaries) g is the pre-stream state and each
+// post-stream population is pulled from it as k_stream pulls it
+// (code/lb3d_advection.F90:109-151, bounce-back from a rock upstream site,
+// rock sites unmoved): the moments pass before (k_stream without STORE)
+// wrote rho, psi and the momenta, and the post-stream populations never go
+// to HBM.  The values are those k_stream would have stored, so f comes out
+// the same bit for bit.
 // ---------------------------------------------------------------------------
-template <int NC, bool LE>
-__global__ void __launch_bounds__(256) k_collide(DevParams P, const double *__restrict__ g,
+template <int NC, bool LE, bool PULL = false, bool ROCK = true>
+__global__ void __launch_bounds__(256, 2) k_collide(DevParams P, const double *__restrict__ g,
                                                  double *__restrict__ f,
                                                  const double *__restrict__ rho,
                                                  const double *__restrict__ psi,
@@ -544,6 +555,7 @@ __global__ void __launch_bounds__(256) k_collide(DevParams P, const double *__re
   double rt = fmaxf_(rho_tilde, CLIP_RHO);
   double ut[3];
   for (int k = 0; k < 3; ++k) ut[k] = pt[k] / rt;
+#pragma unroll
   for (int c = 0; c < NC; ++c) {
     double pon = 1.0 / fmaxf_(r[c], CLIP_RHO);
     double du[3];
@@ -552,7 +564,14 @@ __global__ void __launch_bounds__(256) k_collide(DevParams P, const double *__re
     boltz2(ut[0], ut[1], ut[2], du[0], du[1], du[2], b);
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
-      double nq = g[(c * 19 + q) * N + i];
+      double nq;
+      if (!PULL || q == REST || (ROCK && rock[i] != 0)) {
+        nq = g[(c * 19 + q) * N + i];
+      } else {
+        const long long j =
+            sidx(wrap(x - cx(q), P.nx), wrap(y - cy(q), P.ny), wrap(z - cz(q), P.nz), P.nx, P.ny);
+        nq = (ROCK && rock[j] != 0) ? g[(c * 19 + bounce(q)) * N + i] : g[(c * 19 + q) * N + j];
+      }
       double eq = r[c] * b[q];
       f[(c * 19 + q) * N + i] = nq - P.omega[c] * (nq - eq);
     }
@@ -752,6 +771,61 @@ cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, dou
   }
 #undef LB3D_STREAM
   return cudaSuccess;
+}
+
+cudaError_t fp64_step_pull(const DevParams &P, const double *fin, double *fout, double *rho,
+                           double *psi, double *mom, double *da, double *db, const uint8_t *rock,
+                           cudaStream_t st) {
+  if (P.le || P.zouhe) return cudaErrorInvalidValue;
+  unsigned gr = grid_for(P.nsites, 256);
+  const bool rk = P.any_rock != 0;
+  // moments pass: densities, psi and (surfactant) the advected dipole flux
+  for (int c = 0; c < P.nc; ++c) {
+#define LB3D_MOMENTS(NC_, FLUX_, ROCK_)                                                  \
+  k_stream<NC_, false, FLUX_, ROCK_, false, true><<<gr, 256, 0, st>>>(P, fin, nullptr, rho, psi, \
+                                                                      mom, da, db, rock, nullptr, \
+                                                                      nullptr, c)
+    if (P.nc == 2) {
+      if (rk)
+        LB3D_MOMENTS(2, false, true);
+      else
+        LB3D_MOMENTS(2, false, false);
+    } else if (c < 2) {
+      if (rk)
+        LB3D_MOMENTS(3, false, true);
+      else
+        LB3D_MOMENTS(3, false, false);
+    } else {
+      if (rk)
+        LB3D_MOMENTS(3, true, true);
+      else
+        LB3D_MOMENTS(3, true, false);
+    }
+#undef LB3D_MOMENTS
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (P.nc == 3) {
+    k_dipole<<<grid_for(P.nsites, 256), 256, 0, st>>>(P, rho, da, db);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (P.nc == 2) {
+    if (rk)
+      k_collide<2, false, true, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, db, rock, nullptr,
+                                                           nullptr);
+    else
+      k_collide<2, false, true, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, db, rock, nullptr,
+                                                            nullptr);
+  } else {
+    if (rk)
+      k_collide<3, false, true, true><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, db, rock, nullptr,
+                                                           nullptr);
+    else
+      k_collide<3, false, true, false><<<gr, 256, 0, st>>>(P, fin, fout, rho, psi, mom, db, rock, nullptr,
+                                                            nullptr);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t fp64_dipole(const DevParams &P, const double *rho, const double *da, double *db,

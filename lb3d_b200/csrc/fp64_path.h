@@ -21,6 +21,15 @@ cudaError_t fp64_stream(const DevParams &P, const double *fin, double *fout, dou
                         double *psi, double *mom, double *da, const double *db,
                         const uint8_t *rock, const double *hlo, const double *hhi,
                         cudaStream_t st);
+// One time step with streaming fused into the collision (periodic lattices,
+// no Lees-Edwards planes, no stage-8 boundaries): moments pass (rho, psi,
+// momenta, dipole flux), dipole relaxation (ternary), pull + forces + BGK
+// from fin into fout.  Every buffer ends up as after fp64_stream +
+// fp64_dipole + fp64_collide, bit for bit, except that the post-stream
+// populations are never stored.
+cudaError_t fp64_step_pull(const DevParams &P, const double *fin, double *fout, double *rho,
+                           double *psi, double *mom, double *da, double *db, const uint8_t *rock,
+                           cudaStream_t st);
 cudaError_t fp64_dipole(const DevParams &P, const double *rho, const double *da, double *db,
                         cudaStream_t st);
 cudaError_t fp64_collide(const DevParams &P, const double *g, double *f, const double *rho,
