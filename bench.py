@@ -42,7 +42,7 @@ BYTES_PER_SITE = {("f32", 3): 480, ("f32", 2): 304, ("f64", 3): 960, ("f64", 2):
 # passes; 32x8 tiles).  Keyed by (tile x, tile y, strategy); for strategy 3
 # the tile shape moves only halo reloads that hit L2, so its figure stands
 # for every shape.
-NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 772, (32, 8, 3): 549}
+NCU_TRAFFIC_PER_SITE = {(32, 4, 2): 772, (32, 8, 3): 561}
 
 
 def ncu_traffic(shape):

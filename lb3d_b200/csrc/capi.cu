@@ -197,6 +197,8 @@ DevParams make_dev_params(const lb3dc_params &p) {
   // (code/lb3d_ic_rock.F90:176-183).
   P.rc_r = p.rock_colour_r > 0 ? p.rock_colour_r : 0.0;
   P.rc_b = p.rock_colour_b > 0 ? p.rock_colour_b : 0.0;
+  P.psi_rc[0] = 1.0 - lb3d_detmath::det_exp(-(0.0 + P.rc_r));
+  P.psi_rc[1] = 1.0 - lb3d_detmath::det_exp(-(0.0 + P.rc_b));
   P.le = (p.boundary_cond != 0 && (p.inv_fluid == 5 || p.inv_fluid == 6)) ? 1 : 0;
   P.any_rock = 1;  // until a state without rock is uploaded
   P.zouhe = (p.boundary_cond != 0 && p.inv_fluid == 12) ? 1 : 0;

@@ -45,6 +45,7 @@ struct DevParams {
   int g_accn_min, g_accn_max, g_accn_min_x, g_accn_max_x, g_accn_min_y, g_accn_max_y;
   int inv_fluid;
   double rc_r, rc_b;  // rock colour at rock sites (0 where not set)
+  double psi_rc[2];   // 1 - exp(-rc) (detmath.h), the psi of a rock site whose density is 0
   int le;             // Lees-Edwards on the x-planes
   int any_rock;       // some site is rock (0: the stream kernel skips the rock tests)
   int zouhe;          // Zou-He flux boundaries on the z planes (inv_fluid 12)

@@ -415,8 +415,13 @@ __device__ __forceinline__ void sc_force_binary(const DevParams &P, int x, int y
         bool through_halo = (yn < 0 || yn >= ny || zn < 0 || zn >= nz || xn < 0 || xn >= nx);
         double rcr = (LE && through_halo) ? 0.0 : P.rc_r;
         double rcb = (LE && through_halo) ? 0.0 : P.rc_b;
-        psi_r = get_psi(rho[j] + rcr);
-        psi_b = get_psi(rho[N + j] + rcb);
+        // rock sites hold no populations, so their density is 0 and their
+        // psi is that of the rock colour alone (evaluated once on the host
+        // by the same detmath routine: the same bits)
+        const double rj = rho[j], bj = rho[N + j];
+        const bool coloured = !(LE && through_halo);
+        psi_r = (coloured && rj == 0.0) ? P.psi_rc[0] : get_psi(rj + rcr);
+        psi_b = (coloured && bj == 0.0) ? P.psi_rc[1] : get_psi(bj + rcb);
       } else {
         psi_r = psi[j];
         psi_b = psi[N + j];
@@ -520,7 +525,7 @@ __device__ __forceinline__ void sc_forces(const DevParams &P, int x, int y, int 
 // the same bit for bit.
 // ---------------------------------------------------------------------------
 template <int NC, bool LE, bool PULL = false, bool ROCK = true>
-__global__ void __launch_bounds__(256, 2) k_collide(DevParams P, const double *__restrict__ g,
+__global__ void __launch_bounds__(256, (PULL || NC == 3) ? 2 : 4) k_collide(DevParams P, const double *__restrict__ g,
                                                  double *__restrict__ f,
                                                  const double *__restrict__ rho,
                                                  const double *__restrict__ psi,
@@ -555,8 +560,7 @@ __global__ void __launch_bounds__(256, 2) k_collide(DevParams P, const double *_
   double rt = fmaxf_(rho_tilde, CLIP_RHO);
   double ut[3];
   for (int k = 0; k < 3; ++k) ut[k] = pt[k] / rt;
-#pragma unroll
-  for (int c = 0; c < NC; ++c) {
+  auto bgk = [&](int c) {
     double pon = 1.0 / fmaxf_(r[c], CLIP_RHO);
     double du[3];
     for (int k = 0; k < 3; ++k) du[k] = ((P.tau[c] * pon) * F[c][k]) / P.amass[c];
@@ -565,7 +569,7 @@ __global__ void __launch_bounds__(256, 2) k_collide(DevParams P, const double *_
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
       double nq;
-      if (!PULL || q == REST || (ROCK && rock[i] != 0)) {
+      if (q == REST || (ROCK && rock[i] != 0)) {
         nq = g[(c * 19 + q) * N + i];
       } else {
         const long long j =
@@ -574,6 +578,26 @@ __global__ void __launch_bounds__(256, 2) k_collide(DevParams P, const double *_
       }
       double eq = r[c] * b[q];
       f[(c * 19 + q) * N + i] = nq - P.omega[c] * (nq - eq);
+    }
+  };
+  // unrolled over the components where the pulls fill the loop (keeps r and
+  // F in registers)
+  if constexpr (PULL) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) bgk(c);
+  } else {
+    for (int c = 0; c < NC; ++c) {
+      double pon = 1.0 / fmaxf_(r[c], CLIP_RHO);
+      double du[3];
+      for (int k = 0; k < 3; ++k) du[k] = ((P.tau[c] * pon) * F[c][k]) / P.amass[c];
+      double b[19];
+      boltz2(ut[0], ut[1], ut[2], du[0], du[1], du[2], b);
+#pragma unroll
+      for (int q = 0; q < 19; ++q) {
+        double nq = g[(c * 19 + q) * N + i];
+        double eq = r[c] * b[q];
+        f[(c * 19 + q) * N + i] = nq - P.omega[c] * (nq - eq);
+      }
     }
   }
 }
