@@ -98,6 +98,18 @@ __device__ __forceinline__ void tma_prefetch_desc(const void *tmap) {
   asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
 }
 
+// Programmatic dependent launch between the passes: each pass lets the next
+// one launch once all its CTAs are running (the next pass's CTAs then take
+// the SM resources its finished CTAs free and run their set-up), and waits
+// for the previous grid to complete, with its memory visible, before it
+// reads anything that grid or an earlier one wrote (the lattice
+// descriptors, the fields, the populations).  Without the launch attribute
+// both are no-ops.
+__device__ __forceinline__ void pdl_launch_next() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait_previous() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // Geometry shared by the passes: padded fields with MF_PAD extra sites on
 // each side in x and y (one of them used as the periodic image), ring boxes
 // of the tile plus a one-site halo.
@@ -158,6 +170,8 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
   constexpr int NT = TX * TY, DW = TX + 2, DN = DW * (TY + 2), DR = 4;
   extern __shared__ float4 smd[];  // previous dipoles [DR][DN] (ternary)
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  pdl_launch_next();
+  pdl_wait_previous();
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile T = tiles[t];
     const LatDesc &Lg = lats[T.lat];
@@ -319,6 +333,8 @@ __global__ void __launch_bounds__(TX *TY, 1024 / (TX * TY))
     tma_prefetch_desc(&tm2);
   }
   __syncthreads();
+  pdl_launch_next();
+  pdl_wait_previous();
   auto box = [&](unsigned g) { return reinterpret_cast<const float4 *>(ring + (g % RS) * G::D_SLOT); };
   unsigned gbase = 0, issued = 0, waited = 0;
   bool failed = false;
@@ -494,6 +510,8 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     if (NC == 3) tma_prefetch_desc(&tmd);
   }
   __syncthreads();
+  pdl_launch_next();
+  pdl_wait_previous();
   auto box = [&](unsigned g, int f) {
     return reinterpret_cast<const float4 *>(ring + (g % RS) * G::C_SLOT + f * G::FIELD);
   };
@@ -634,23 +652,22 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
             vz[c] = fmaf(kf, Fx[c][2], u2);
           }
           float *fo = Fo + self;
+          // a site on the sheared x boundary also writes the next step's
+          // pre-stream boundary plane for its stage-6 halo kernel, with the
+          // same equilibrium values (one store sequence for every lane; at
+          // x = 0 and x = nx - 1 both when the lattice is one site wide)
+          float *b0 = nullptr;
+          int NP = 0;
           if (LE && (gx == 0 || gx == nx - 1)) {
-            // a site on the sheared x boundary also writes the next step's
-            // pre-stream boundary plane for its stage-6 halo kernel (at
-            // x = 0 and x = nx - 1 both when the lattice is one site wide)
-            const int NP = ny * nz, o = gy + ny * gz;
-            float *b0 = Lg.le_b[gx == nx - 1 ? 0 : 1] + o;
-            eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
-                      make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
-                      make_float2(Lg.omega[0], Lg.omega[1]), b0, b0 + 19 * NP, (unsigned)NP);
-            if (gx == 0 && gx == nx - 1) {
-              float *b1 = Lg.le_b[1] + o;
-              eq_store2(b1, b1 + 19 * NP, (unsigned)NP, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
-                        make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
-                        make_float2(Lg.omega[0], Lg.omega[1]));
-            }
-          } else {
-            eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+            NP = ny * nz;
+            b0 = Lg.le_b[gx == nx - 1 ? 0 : 1] + gy + ny * gz;
+          }
+          eq_store2(fo, fo + (size_t)19 * S, S, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
+                    make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
+                    make_float2(Lg.omega[0], Lg.omega[1]), b0, b0 ? b0 + 19 * NP : nullptr, (unsigned)NP);
+          if (LE && gx == 0 && gx == nx - 1) {
+            float *b1 = Lg.le_b[1] + gy + ny * gz;
+            eq_store2(b1, b1 + 19 * NP, (unsigned)NP, make_float2(rho[0], rho[1]), make_float2(dr[0], dr[1]),
                       make_float2(vx[0], vx[1]), make_float2(vy[0], vy[1]), make_float2(vz[0], vz[1]),
                       make_float2(Lg.omega[0], Lg.omega[1]));
           }

@@ -1066,9 +1066,9 @@ cudaError_t fp32_launch_fused(int nc, bool rock, bool body, const FusedShape &sh
   if (le) {
     // stage 6 halo, moments pass, stage 8 halo, staged collide pass
     if (!P || nc != 2 || sh.split != 2 || !M) return cudaErrorInvalidValue;
-    // one thread per (y, z) of the x-halo planes: 64-thread blocks spread
-    // the few thousand threads over every SM
-    const unsigned g = (unsigned)((P->ny * P->nz + 63) / 64);
+    // two threads per (y, z) of the x-halo planes (one per side): 64-thread
+    // blocks spread the few thousand threads over every SM
+    const unsigned g = (unsigned)((2 * P->ny * P->nz + 63) / 64);
     k_le_pre32<2><<<g, 64, 0, st>>>(*P, *le, d_lat, f0, f1, S);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
@@ -1316,6 +1316,27 @@ static size_t mf_smem(int nc, int tx, int ty, int which) {
 // collide pass, each on its own tile list and resident grid; with le (a
 // binary Lees-Edwards lattice) the stage-6 halo kernel runs before the
 // moments pass and the stage-8 one before the collide pass.
+// One pass of strategy 3, launched with programmatic stream serialization
+// (pdl): its CTAs may start while the previous kernel on the stream
+// finishes, and wait for it before reading its results (pdl_wait_previous).
+// Lattices with rock launch plainly (the overlap measured 0.8 % slower on
+// the porous lattice, 0.9-1 % faster on the periodic and sheared ones).
+static cudaError_t launch_pdl(const void *fn, dim3 grid, dim3 block, void **args, size_t smem,
+                              cudaStream_t st, bool pdl) {
+  if (!pdl) return cudaLaunchKernel(fn, grid, block, args, smem, st);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *rockp, cudaStream_t st,
                              const LEStep *le) {
   const bool rock = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
@@ -1325,7 +1346,7 @@ static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *ro
   if (!mf_fns(P.nc, rock, body, s.tx, s.ty, narrow, &fn[0], &fn[1], &fn[2], le != nullptr))
     return cudaErrorInvalidConfiguration;
   if (le && !s.le_h[0]) return cudaErrorInvalidValue;
-  const unsigned leg = (unsigned)((P.ny * P.nz + 63) / 64);
+  const unsigned leg = (unsigned)((2 * P.ny * P.nz + 63) / 64);  // two threads per (y, z)
   if (s.mf_tx != s.tx || s.mf_ty != s.ty || !s.mf_tiles) return cudaErrorInvalidConfiguration;
   const int nt = s.tx * s.ty;
   const LatDesc *dl = s.d_lat;
@@ -1351,18 +1372,18 @@ static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *ro
       void *args[] = {(void *)&dl, (void *)&dt, (void *)&ntl, (void *)&f0, (void *)&f1, (void *)&d0,
                       (void *)&d1, (void *)&rockp, (void *)&S, (void *)&s.MF1, (void *)&s.MF2,
                       (void *)&s.MFp, (void *)&s.DS};
-      e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
+      e = launch_pdl(fn[pass], grid, dim3(nt), args, sm, st, !rock);
     } else if (pass == 1) {
       const float *ds = s.DS;
       void *args[] = {(void *)&s.tm2, (void *)&dl, (void *)&dt, (void *)&ntl, (void *)&s.db[0],
                       (void *)&s.db[1], (void *)&ds, (void *)&s.DD, (void *)&s.err};
-      e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
+      e = launch_pdl(fn[pass], grid, dim3(nt), args, sm, st, !rock);
     } else {
       const float2 *mfp = s.MFp;
       void *args[] = {(void *)&s.tm1, (void *)&s.tmd, (void *)&dl, (void *)&dt, (void *)&ntl,
                       (void *)&s.f[0], (void *)&s.f[1], (void *)&s.db[0], (void *)&s.db[1], (void *)&rockp,
                       (void *)&S, (void *)&mfp, (void *)&s.err};
-      e = cudaLaunchKernel(fn[pass], grid, dim3(nt), args, sm, st);
+      e = launch_pdl(fn[pass], grid, dim3(nt), args, sm, st, !rock);
     }
   }
   return e;

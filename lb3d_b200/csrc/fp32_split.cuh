@@ -551,9 +551,10 @@ __global__ void __launch_bounds__(TX *TY, Collide2Geom<NC, TX, TY>::MINB)
 
 
 // ---------------------------------------------------------------------------
-// Lees-Edwards x-halos of the FP32 path (binary single lattices), one
-// thread per (y, z), in FP64 from the FP32 deviations with the FP64 path's
-// adjustment (le_adjust: the equilibrium shift by -/+ 2 shear_u along z,
+// Lees-Edwards x-halos of the FP32 path (binary single lattices), two
+// threads per (y, z), one per halo side, in FP64 from the FP32 deviations
+// with the FP64 path's adjustment (le_adjust: the equilibrium shift by -/+
+// 2 shear_u along z,
 // the clipping rule and the top halo's reading of the adjusted bottom site,
 // code/lb3d_bc_leesedwards.F90:147-1315).
 //   k_le_pre32  (stage 6): pre-stream populations at x = nx - 1 / x = 0,
@@ -571,18 +572,22 @@ template <int NC>
 __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ lat,
                            const float *__restrict__ f0, const float *__restrict__ f1, unsigned S) {
   const LatDesc &Lg = *lat;
-  const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
+  const int ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= NP) return;
-  const int y = t % ny, z = t / ny;
-  const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base;
+  if (t >= 2 * NP) return;
+  // threads [0, NP) build the bottom halo site of (y, z), threads [NP, 2 NP)
+  // the top one (consecutive threads read consecutive y)
+  const bool top = t >= NP;
+  const int u = top ? t - NP : t;
+  const int y = u % ny, z = u / ny;
   const double rho0 = (double)Lg.rho0, f = L.lefrac;
-  double hb[NC][19], ht[NC][19];
-  // the pre-stream populations of x = nx - 1 and x = 0 come from the compact
-  // boundary planes (consecutive threads read consecutive y)
-  (void)F;
+  (void)f0;
+  (void)f1;
   (void)S;
-  {
+  // the pre-stream populations of x = nx - 1 and x = 0 come from the compact
+  // boundary planes
+  double hb[NC][19];
+  auto bottom = [&]() {
     const int ia = y + ny * wrapz(z + L.eoff, nz), ib = y + ny * wrapz(z + L.eoff + 1, nz);
     const float *B = Lg.le_b[0];
     for (int c = 0; c < NC; ++c)
@@ -592,7 +597,15 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
                    f * ((double)B[(c * 19 + q) * NP + ib] + w);
       }
     le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
+  };
+  if (!top) {
+    bottom();
+    for (int c = 0; c < NC; ++c)
+      for (int q = 0; q < 19; ++q)
+        Lg.le_h[0][(c * 19 + q) * NP + u] = (float)(hb[c][q] - __dmul_rn(wq64(q), rho0));
+    return;
   }
+  double ht[NC][19], df[NC][19];
   {
     const int ia = y + ny * wrapz(z - L.eoff - 1, nz), ib = y + ny * wrapz(z - L.eoff, nz);
     const float *B = Lg.le_b[1];
@@ -602,14 +615,15 @@ __global__ void k_le_pre32(DevParams P, LEStep L, const LatDesc *__restrict__ la
         ht[c][q] = f * ((double)B[(c * 19 + q) * NP + ia] + w) +
                    (1.0 - f) * ((double)B[(c * 19 + q) * NP + ib] + w);
       }
-    le_adjust<NC>(P, ht, hb, L.shear_u, +1.0);
   }
+  // the top site's clipping rule reads the adjusted bottom site, which this
+  // thread builds only when the rule applies
+  const bool neg = le_adjust_df<NC>(P, ht, L.shear_u, +1.0, df);
+  if (neg) bottom();
+  le_adjust_apply<NC>(ht, hb, df, neg);
   for (int c = 0; c < NC; ++c)
-    for (int q = 0; q < 19; ++q) {
-      const double w = __dmul_rn(wq64(q), rho0);
-      Lg.le_h[0][(c * 19 + q) * NP + t] = (float)(hb[c][q] - w);
-      Lg.le_h[1][(c * 19 + q) * NP + t] = (float)(ht[c][q] - w);
-    }
+    for (int q = 0; q < 19; ++q)
+      Lg.le_h[1][(c * 19 + q) * NP + u] = (float)(ht[c][q] - __dmul_rn(wq64(q), rho0));
 }
 
 template <int NC>
@@ -618,49 +632,61 @@ __global__ void k_le_post32(DevParams P, LEStep L, const LatDesc *__restrict__ l
   const LatDesc &Lg = *lat;
   const int nx = Lg.nx, ny = Lg.ny, nz = Lg.nz, NP = ny * nz;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= NP) return;
-  const int y = t % ny, z = t / ny;
-  const float *__restrict__ F = (Lg.parity ? f1 : f0) + Lg.base;
+  if (t >= 2 * NP) return;
+  const bool top = t >= NP;
+  const int u = top ? t - NP : t;
+  const int y = u % ny, z = u / ny;
   const double rho0 = (double)Lg.rho0, f = L.lefrac;
+  (void)f0;
+  (void)f1;
+  (void)S;
   // post-stream population q of component c at (x, yy, zz), x = nx - 1 or
   // 0: the moments pass left them in the compact boundary planes, pulled as
   // it pulls every site (across x from the stage-6 halo planes)
-  (void)F;
-  (void)S;
   auto post = [&](int c, int q, int x, int yy, int zz) -> double {
     const float v = Lg.le_b[x == 0 ? 3 : 2][(c * 19 + q) * NP + yy + ny * zz];
     return (double)v + __dmul_rn(wq64(q), rho0);
   };
-  double hb[NC][19], ht[NC][19];
-  {
+  double hb[NC][19];
+  auto bottom = [&]() {
     const int za = wrapz(z + L.eoff, nz), zb = wrapz(z + L.eoff + 1, nz);
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q)
         hb[c][q] = (1.0 - f) * post(c, q, nx - 1, y, za) + f * post(c, q, nx - 1, y, zb);
     le_adjust<NC>(P, hb, hb, L.shear_u, -1.0);
+  };
+  // psi(rho) - psi(rho0) = -e^{-rho0} expm1(-(rho - rho0)) of each
+  // component's density at the halo site h
+  const double em0 = exp(-rho0);
+  auto dpsi = [&](const double h[NC][19], double d[NC]) {
+    for (int c = 0; c < NC; ++c) {
+      double a = 0.0;
+#pragma unroll
+      for (int q = 0; q < 19; ++q) a = a + h[c][q] * (double)gw(q);
+      d[c] = -em0 * expm1(-(a - rho0));
+    }
+  };
+  double d[NC];
+  if (!top) {
+    bottom();
+    dpsi(hb, d);
+    Lg.le_p[0][u] = make_float2((float)d[0], (float)d[1]);
+    return;
   }
+  double ht[NC][19], df[NC][19];
   {
     const int za = wrapz(z - L.eoff - 1, nz), zb = wrapz(z - L.eoff, nz);
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q)
         ht[c][q] = f * post(c, q, 0, y, za) + (1.0 - f) * post(c, q, 0, y, zb);
-    le_adjust<NC>(P, ht, hb, L.shear_u, +1.0);
   }
-  double dl[NC], dh[NC];
-  const double em0 = exp(-rho0);
-  for (int c = 0; c < NC; ++c) {
-    double a = 0.0, b = 0.0;
-#pragma unroll
-    for (int q = 0; q < 19; ++q) {
-      a = a + hb[c][q] * (double)gw(q);
-      b = b + ht[c][q] * (double)gw(q);
-    }
-    // psi(rho) - psi(rho0) = -e^{-rho0} expm1(-(rho - rho0))
-    dl[c] = -em0 * expm1(-(a - rho0));
-    dh[c] = -em0 * expm1(-(b - rho0));
-  }
-  Lg.le_p[0][t] = make_float2((float)dl[0], (float)dl[1]);
-  Lg.le_p[1][t] = make_float2((float)dh[0], (float)dh[1]);
+  // the top site's clipping rule reads the adjusted bottom site, built here
+  // only when the rule applies
+  const bool neg = le_adjust_df<NC>(P, ht, L.shear_u, +1.0, df);
+  if (neg) bottom();
+  le_adjust_apply<NC>(ht, hb, df, neg);
+  dpsi(ht, d);
+  Lg.le_p[1][u] = make_float2((float)d[0], (float)d[1]);
 }
 
 // Fills the compact pre-stream boundary planes from the state (after an

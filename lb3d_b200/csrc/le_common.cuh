@@ -56,9 +56,12 @@ __device__ __forceinline__ void boltz2(double ux, double uy, double uz, double d
 // clipping branch of the top halo reads the adjusted bottom site
 // (:951-986).
 // ---------------------------------------------------------------------------
+// The first half of the adjustment: the equilibrium shift df of the halo
+// site h; returns whether h + df would go negative somewhere, the case in
+// which the clipping rule reads the reference site.
 template <int NC>
-__device__ void le_adjust(const DevParams &P, double h[NC][19], const double ref[NC][19],
-                          double shear_u, double sign) {
+__device__ bool le_adjust_df(const DevParams &P, const double h[NC][19], double shear_u, double sign,
+                             double df[NC][19]) {
   double p[NC][3], ns[NC];
   for (int c = 0; c < NC; ++c) {
     ns[c] = 0.0;
@@ -89,7 +92,6 @@ __device__ void le_adjust(const DevParams &P, double h[NC][19], const double ref
   double uz2 = (sign < 0.0) ? ((ut[2] - shear_u) - shear_u) : ((ut[2] + shear_u) + shear_u);
   boltz2(ut[0], ut[1], uz2, 0.0, 0.0, 0.0, b_udu);
   boltz2(ut[0], ut[1], ut[2], 0.0, 0.0, 0.0, b_u);
-  double df[NC][19];
   bool neg = false;
   for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -97,6 +99,14 @@ __device__ void le_adjust(const DevParams &P, double h[NC][19], const double ref
       df[c][q] = ns[c] * (b_udu[q] - b_u[q]);
       if (h[c][q] + df[c][q] < 0.0) neg = true;
     }
+  return neg;
+}
+
+// The second half: h + df, or, when that goes negative, the reference site
+// plus df scaled to keep it non-negative (ref is read only then).
+template <int NC>
+__device__ void le_adjust_apply(double h[NC][19], const double ref[NC][19], const double df[NC][19],
+                                bool neg) {
   if (neg) {
     double mn = ref[0][0];
     for (int c = 0; c < NC; ++c)
@@ -120,6 +130,14 @@ __device__ void le_adjust(const DevParams &P, double h[NC][19], const double ref
     for (int c = 0; c < NC; ++c)
       for (int q = 0; q < 19; ++q) h[c][q] = h[c][q] + df[c][q];
   }
+}
+
+template <int NC>
+__device__ void le_adjust(const DevParams &P, double h[NC][19], const double ref[NC][19],
+                          double shear_u, double sign) {
+  double df[NC][19];
+  const bool neg = le_adjust_df<NC>(P, h, shear_u, sign, df);
+  le_adjust_apply<NC>(h, ref, df, neg);
 }
 
 }  // namespace lb3d
