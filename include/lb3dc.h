@@ -144,7 +144,12 @@ int lb3dc_advection(lb3dc_handle *h);
 /* code/lb3d_collision.F90:41-291: dipole relaxation (ternary), Shan-Chen
  * and body forces, BGK relaxation. */
 int lb3dc_collision(lb3dc_handle *h);
-/* nsteps full time steps (stages 6..9 each); may fuse stages. */
+/* nsteps full time steps (stages 6..9 each); may fuse stages.  The FP64
+ * path pulls the post-stream populations inside its collision kernel where
+ * nothing acts on them between advection and collision (no Lees-Edwards
+ * planes, no inflow boundaries): the results, rho, psi, the momenta and the
+ * dipole flux included, are those of the stage-by-stage calls bit for
+ * bit. */
 int lb3dc_time_loop(lb3dc_handle *h, int nsteps);
 /* Waits for all work of h; reports deferred kernel errors. */
 int lb3dc_sync(lb3dc_handle *h);
@@ -163,9 +168,9 @@ int lb3dc_sync(lb3dc_handle *h);
  * collide pass that receive those fields as TMA boxes with a one-site halo,
  * the collide pass writing the equilibrium: offered only when every
  * component relaxes fully (tau = 1) on a lattice at least 2 sites across in
- * x and y without Lees-Edwards planes or inflow boundaries (LB3DC_ENOTSUP
- * otherwise); each of its passes chunks z to fill its own resident grid, so
- * zc is not used.  All strategies give the same result up to FP32
+ * x and y without inflow boundaries (LB3DC_ENOTSUP otherwise); each of its
+ * passes chunks z to fill its own resident grid, so zc is not used.
+ * Lees-Edwards lattices (binary) run strategies 2 and 3 only.  All strategies give the same result up to FP32
  * rounding; 0, 1, 2 and 3 agree bit for bit (up to the sign of zero). */
 int lb3dc_set_launch_shape(lb3dc_handle *h, int tx, int ty, int zc, int split);
 int lb3dc_get_launch_shape(const lb3dc_handle *h, int *tx, int *ty, int *zc, int *split);
