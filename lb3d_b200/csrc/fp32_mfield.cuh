@@ -491,9 +491,9 @@ __device__ __forceinline__ void force_ternary_pre(const float2 *Pm, const float2
 template <int NC, int TX, int TY, bool ROCK, bool BODY, bool LE = false>
 __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
     k_mf_collide(const __grid_constant__ CUtensorMap tm1, const __grid_constant__ CUtensorMap tmd,
-                 const LatDesc *lats, const Tile *__restrict__ tiles, int ntiles, float *f0,
+                 const LatDesc *__restrict__ lats, const Tile *__restrict__ tiles, int ntiles, float *f0,
                  float *f1, const float *db0, const float *db1, const uint8_t *__restrict__ rock, unsigned S,
-                 const float2 *__restrict__ MFp, int *err, LatDesc *flip) {
+                 const float2 *__restrict__ MFp, int *err) {
   using G = MfGeom<NC, TX, TY>;
   constexpr int AW = G::AW, AN = G::AN, RS = G::C_RS, PR = G::PR, AHEAD = G::AHEAD;
   extern __shared__ unsigned char smraw_[];
@@ -689,20 +689,5 @@ __global__ void __launch_bounds__(TX *TY, MfGeom<NC, TX, TY>::C_MINB)
       for (unsigned g = waited; g < issued; ++g) mbar_wait_bounded(&bars[g % RS], (g / RS) & 1u);
     }
     __syncthreads();
-  }
-  if (flip) {
-    // the step's parity flip (a single lattice): err[1] counts the CTAs that
-    // are done with the lattice descriptor, and the last one flips the
-    // parity the next step reads, then resets the count
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      unsigned *done = reinterpret_cast<unsigned *>(err + 1);
-      if (atomicAdd(done, 1u) == gridDim.x - 1) {
-        if (flip->flags & LAT_ACTIVE) flip->parity ^= 1;
-        *done = 0u;
-        __threadfence();
-      }
-    }
   }
 }

@@ -1206,9 +1206,7 @@ static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
   if (ok && P.nc == 3) ok = cudaMalloc(&s.DD, plane) == cudaSuccess;
   if (ok) ok = cudaMalloc(&s.MFp, (size_t)P.nsites * sizeof(float2)) == cudaSuccess;
   if (ok && P.nc == 3) ok = cudaMalloc(&s.DS, (size_t)P.nsites * sizeof(float)) == cudaSuccess;
-  // err[0]: a bounded wait that gave up; err[1]: the collide pass's count of
-  // finished CTAs (its last CTA flips the parity)
-  if (ok && !s.err) ok = cudaMalloc(&s.err, 2 * sizeof(int)) == cudaSuccess;
+  if (ok && !s.err) ok = cudaMalloc(&s.err, sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     if (s.MF1) cudaFree(s.MF1);
@@ -1225,7 +1223,7 @@ static int ensure_mf(const DevParams &P, Fp32State &s, cudaStream_t st) {
   cudaMemsetAsync(s.MF1, 0, plane, st);
   if (s.MF2) cudaMemsetAsync(s.MF2, 0, plane, st);
   if (s.DD) cudaMemsetAsync(s.DD, 0, plane, st);
-  cudaMemsetAsync(s.err, 0, 2 * sizeof(int), st);
+  cudaMemsetAsync(s.err, 0, sizeof(int), st);
   s.bytes += (long long)plane * (P.nc == 3 ? 3 : 1) + P.nsites * (P.nc == 3 ? 12 : 8);
   return LB3DC_OK;
 }
@@ -1382,10 +1380,9 @@ static cudaError_t launch_mf(const DevParams &P, Fp32State &s, const uint8_t *ro
       e = launch_pdl(fn[pass], grid, dim3(nt), args, sm, st, !rock);
     } else {
       const float2 *mfp = s.MFp;
-      LatDesc *flip = s.d_lat;  // the collide pass flips the parity at its end
       void *args[] = {(void *)&s.tm1, (void *)&s.tmd, (void *)&dl, (void *)&dt, (void *)&ntl,
                       (void *)&s.f[0], (void *)&s.f[1], (void *)&s.db[0], (void *)&s.db[1], (void *)&rockp,
-                      (void *)&S, (void *)&mfp, (void *)&s.err, (void *)&flip};
+                      (void *)&S, (void *)&mfp, (void *)&s.err};
       e = launch_pdl(fn[pass], grid, dim3(nt), args, sm, st, !rock);
     }
   }
@@ -1882,10 +1879,9 @@ int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, 
   FusedShape sh{s.tx, s.ty, s.zc, s.split};
   const bool rk = (s.lat.flags & LAT_ROCK) != 0, body = (s.lat.flags & LAT_BODY) != 0;
   if (le && !s.le_h[0]) return LB3DC_ESTATE;
-  // kernels per step: the pass(es), two Lees-Edwards halo kernels, the parity
-  // flip (done by the last CTA of the collide pass in strategy 3)
+  // kernels per step: the pass(es), two Lees-Edwards halo kernels, the parity flip
   const int passes = sh.split ? (P.nc == 3 ? 3 : 2) : 1;
-  const int per_step = passes + (le ? 2 : 0) + (sh.split == 3 ? 0 : 1);
+  const int per_step = passes + (le ? 2 : 0) + 1;
   for (int i = 0; i < nsteps; ++i) {
     if (s.timer) s.timer->start(st);
     cudaError_t e = sh.split == 3
@@ -1898,10 +1894,8 @@ int fp32_run(const DevParams &P, Fp32State &s, const uint8_t *rock, int nsteps, 
       s.timer->launches += per_step;
     }
     if (e != cudaSuccess) return LB3DC_ECUDA;
-    if (sh.split != 3) {
-      e = fp32_flip_parity(s.d_lat, 1, st);
-      if (e != cudaSuccess) return LB3DC_ECUDA;
-    }
+    e = fp32_flip_parity(s.d_lat, 1, st);
+    if (e != cudaSuccess) return LB3DC_ECUDA;
     s.lat.parity ^= 1;
   }
   return LB3DC_OK;

@@ -78,9 +78,8 @@ struct Fp32State {
   float *le_b[4] = {nullptr, nullptr, nullptr, nullptr};
   // moment-field strategy (split 3): the halo-padded moment fields (and
   // dipole field, ternary), the plain momentum plane, the tensor maps of their
-  // TMA boxes (encoded for the tile shape mf_tx x mf_ty) and two device
-  // words: err[0] flags a wait that gave up, err[1] counts the collide
-  // pass's finished CTAs (its last CTA flips the parity)
+  // TMA boxes (encoded for the tile shape mf_tx x mf_ty) and the device flag
+  // of a wait that gave up
   float4 *MF1 = nullptr, *MF2 = nullptr, *DD = nullptr;
   float2 *MFp = nullptr;
   float *DS = nullptr;
