@@ -1179,7 +1179,7 @@ long long fp32_footprint(const lb3dc_params &p) {
                                    : 0;
   return 2LL * p.ncomp * 19 * N * 4 + (p.ncomp == 3 ? 6LL * N * 4 : 0) +
          N * fp32_moment_bytes(p.ncomp) + mf +
-         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) + 4 * np * p.ncomp * 19 * 4 : 0) + N * 8 + 4096;
+         (le ? 2 * np * (p.ncomp * 19 * 4 + 8) + 4 * np * p.ncomp * 19 * 4 : 0) + N * 16 + 4096;
 }
 
 // ---------------------------------------------------------------------------
