@@ -522,10 +522,13 @@ __device__ __forceinline__ void sc_forces(const DevParams &P, int x, int y, int 
 // rock sites unmoved): the moments pass before (k_stream without STORE)
 // wrote rho, psi and the momenta, and the post-stream populations never go
 // to HBM.  The values are those k_stream would have stored, so f comes out
-// the same bit for bit.
+// the same bit for bit.  Occupancy (measured): the pulling variants run 2
+// CTAs of 256 threads per SM, the binary one with rock 3 (faster despite
+// its spills: 8.4 against 9.2 ms per step on a 256^3 porous lattice, where
+// the ternary one at 3 ran 15 % slower), the staged binary ones 4.
 // ---------------------------------------------------------------------------
 template <int NC, bool LE, bool PULL = false, bool ROCK = true>
-__global__ void __launch_bounds__(256, (PULL || NC == 3) ? 2 : 4) k_collide(DevParams P, const double *__restrict__ g,
+__global__ void __launch_bounds__(256, (PULL && ROCK && NC == 2) ? 3 : ((PULL || NC == 3) ? 2 : 4)) k_collide(DevParams P, const double *__restrict__ g,
                                                  double *__restrict__ f,
                                                  const double *__restrict__ rho,
                                                  const double *__restrict__ psi,
