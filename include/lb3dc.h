@@ -316,10 +316,10 @@ long long lb3dc_ensemble_bytes(const lb3dc_ensemble *e);
 
 /* ---- FP64 step without device allocation ------------------------------ */
 /* No counterpart in the reference.  For callers that may not call
- * cudaMalloc -- code running while a stream is captured into a CUDA graph,
- * hosts that own all device memory through their own pool or arrays (for
- * instance a Fortran code keeping its lattice in its own device arrays), or
- * loops that cannot take the synchronisation an allocation can imply.
+ * cudaMalloc -- hosts that own all device memory through their own pool or
+ * arrays (for instance a Fortran code keeping its lattice in its own device
+ * arrays, or a server that fixes its HBM budget at start-up), or loops that
+ * cannot take the synchronisation an allocation can imply.
  * Runs nsteps periodic FP64 steps (the same kernels and results as
  * lb3dc_time_loop with precision LB3DC_FP64) on device buffers the caller
  * owns:

@@ -1,12 +1,11 @@
 // noalloc.cu -- the FP64 time step for callers that cannot allocate device
 // memory.
 //
-// Some callers may not call cudaMalloc: code that runs while a CUDA stream
-// is being captured into a graph (allocation is not a capturable stream
-// operation), hosts that own every device byte through their own pool or
-// allocator (a Fortran code holding its lattice in its own device arrays, a
-// server that fixes its HBM budget at start-up) and loops that cannot afford
-// the device-wide synchronisation an allocation can imply.  For them,
+// Some callers may not call cudaMalloc: hosts that own every device byte
+// through their own pool or allocator (a Fortran code holding its lattice in
+// its own device arrays, a server that fixes its HBM budget at start-up) and
+// loops that cannot afford the device-wide synchronisation an allocation can
+// imply.  For them,
 // lb3dc_time_loop_fp64_noalloc runs the FP64 drop-in step on buffers the
 // caller owns and keeps its intermediate fields (the post-stream populations
 // and moments) in a file-scope device array of fixed size instead of

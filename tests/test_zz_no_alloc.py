@@ -1,8 +1,7 @@
 """The FP64 step without device allocation (lb3dc_time_loop_fp64_noalloc).
 
-Callers that may not call cudaMalloc (while a stream is being captured into
-a graph, or when every device byte is owned by the caller's own pool or
-arrays) hand the step their own device buffers; its scratch lives in a
+Callers that may not call cudaMalloc (every device byte owned by the
+caller's own pool or arrays) hand the step their own device buffers; its scratch lives in a
 fixed-size device array inside the library.  Its results must be those of
 the allocating entry point: the FP64 path is exact, so the comparison is
 exact, over two calls in a row (the scratch array keeps the previous call's
